@@ -1,0 +1,264 @@
+"""cudakdtree_b200 -- B200-native k-d trees behind the C ABI of libcukd_b200.so.
+
+Python mirror of the reference's host API (ingowald/cudaKDTree):
+
+=======================  ==================================================
+reference (C++ template)  here
+=======================  ==================================================
+cukd::buildTree           build_tree(points, ...)           (builder.h:108)
+buildTree_thrust/...      build_tree(..., builder="thrust") (builder_*.h)
+cukd::computeBounds       compute_bounds(points)            (builder_common.h:151)
+stackBased/stackFree/cct  fcp(tree, queries, method=...)    (fcp.h:54-163)
+  ::fcp
+... ::knn                 knn(tree, queries, k, method=...) (knn.h:83-199)
+=======================  ==================================================
+
+Device memory is handled with torch CUDA tensors; every call goes through
+the compiled library (there is no CPU fallback: importing works without a
+GPU, but calling without the built library or a GPU raises).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+
+import torch
+
+__all__ = [
+    "lib", "Layout", "layout_for", "build_tree", "compute_bounds", "fcp", "knn",
+    "knn_visits", "morton_order", "CukdError", "STACK_BASED", "STACK_FREE", "CCT",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcukd_b200.so")
+
+FLOAT32, INT32 = 0, 1
+STACK_BASED, STACK_FREE, CCT = 0, 1, 2
+METHODS = {"stack_based": STACK_BASED, "stackBased": STACK_BASED, "stack_free": STACK_FREE,
+           "stackFree": STACK_FREE, "cct": CCT}
+BUILDERS = {"default": 0, "thrust": 1, "bitonic": 2, "inplace": 3, "inPlace": 3}
+QUERY_MORTON, QUERY_HEAP_ORDER, QUERY_FORCE_HEAP = 1, 2, 4
+INT64_MAX = (1 << 63) - 1
+
+
+class CukdError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        msg = _status_string(status)
+        if status == 4:
+            msg += f" ({lib().cukd_last_cuda_error().decode()})"
+        super().__init__(f"{what}: {msg} [status {status}]")
+
+
+class Layout(C.Structure):
+    """cukd_layout: the C-ABI form of the reference's data_traits."""
+    _fields_ = [("scalar_type", C.c_int32), ("num_dims", C.c_int32), ("stride", C.c_int32),
+                ("point_offset", C.c_int32), ("dim_offset", C.c_int32),
+                ("dim_shift", C.c_int32), ("dim_bits", C.c_int32)]
+
+    @property
+    def explicit_dim(self):
+        return self.dim_offset >= 0
+
+    def __repr__(self):
+        return (f"Layout(scalar={self.scalar_type}, D={self.num_dims}, stride={self.stride}, "
+                f"poff={self.point_offset}, doff={self.dim_offset}, "
+                f"dshift={self.dim_shift}, dbits={self.dim_bits})")
+
+
+class QueryParams(C.Structure):
+    _fields_ = [("method", C.c_int32), ("k", C.c_int32), ("cutoff_radius", C.c_float),
+                ("eps", C.c_float), ("cutoff_d2", C.c_int64), ("flags", C.c_int32),
+                ("block_size", C.c_int32)]
+
+
+def layout_for(scalar="float32", num_dims=3, stride=None, point_offset=0, dim_offset=-1,
+               dim_shift=0, dim_bits=32):
+    sc = {"float32": FLOAT32, "float": FLOAT32, "int32": INT32, "int": INT32,
+          FLOAT32: FLOAT32, INT32: INT32}[scalar]
+    if stride is None:
+        stride = 4 * num_dims
+    return Layout(sc, num_dims, stride, point_offset, dim_offset, dim_shift, dim_bits)
+
+
+_lib = None
+
+
+def lib():
+    """The compiled library.  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} not built; run `make -C cudakdtree_b200/csrc` "
+                "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        P, I64 = C.c_void_p, C.c_int64
+        L.cukd_build_tree.argtypes = [P, I64, C.POINTER(Layout), P, C.c_int, P, P]
+        L.cukd_compute_bounds.argtypes = [P, I64, C.POINTER(Layout), P, P]
+        L.cukd_fcp.argtypes = [P, I64, C.POINTER(Layout), P, P, I64, C.POINTER(QueryParams), P,
+                               P, P, P]
+        L.cukd_knn.argtypes = [P, I64, C.POINTER(Layout), P, P, I64, C.POINTER(QueryParams), P,
+                               P, P, P, P]
+        L.cukd_knn_visits.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
+                                      C.POINTER(QueryParams), P, P, P]
+        L.cukd_morton_order.argtypes = [P, I64, C.c_int, P, P, P, P]
+        L.cukd_query_params_init.argtypes = [C.POINTER(QueryParams)]
+        L.cukd_status_string.argtypes = [C.c_int]
+        L.cukd_status_string.restype = C.c_char_p
+        L.cukd_last_cuda_error.restype = C.c_char_p
+        for name in ("cukd_build_float2", "cukd_build_float3", "cukd_build_float4",
+                     "cukd_build_int2", "cukd_build_int3", "cukd_build_int4"):
+            getattr(L, name).argtypes = [P, I64, P, P, P]
+        _lib = L
+    return _lib
+
+
+def _status_string(status):
+    try:
+        return lib().cukd_status_string(status).decode()
+    except Exception:  # pragma: no cover
+        return "status"
+
+
+def _check(status, what):
+    if status != 0:
+        raise CukdError(status, what)
+
+
+def _stream(stream):
+    if stream is None:
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, torch.cuda.Stream):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(stream)
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def infer_layout(points: torch.Tensor) -> Layout:
+    """Layout of a plain [n, D] float32/int32 tensor (default_data_traits)."""
+    if points.dim() != 2:
+        raise ValueError("points must be [n, D] for an inferred layout")
+    sc = {torch.float32: FLOAT32, torch.int32: INT32}[points.dtype]
+    return layout_for(sc, points.shape[1])
+
+
+def _num_records(points, layout):
+    return points.numel() * points.element_size() // layout.stride
+
+
+def _bounds_dtype(layout):
+    return torch.float32 if layout.scalar_type == FLOAT32 else torch.int32
+
+
+def compute_bounds(points, layout=None, stream=None):
+    layout = layout or infer_layout(points)
+    n = _num_records(points, layout)
+    wb = torch.empty((2, layout.num_dims), dtype=_bounds_dtype(layout), device=points.device)
+    _check(lib().cukd_compute_bounds(_ptr(points), n, C.byref(layout), _ptr(wb),
+                                     _stream(stream)), "cukd_compute_bounds")
+    return wb
+
+
+def build_tree(points, layout=None, world_bounds=None, builder="default", stream=None,
+               n=None, want_bounds=True):
+    """Builds a left-balanced k-d tree IN PLACE over `points` (a contiguous
+    CUDA tensor holding n records of `layout`).  Returns the world bounds
+    tensor [2, D] (or None when want_bounds is False and the layout has no
+    explicit dims)."""
+    layout = layout or infer_layout(points)
+    if not points.is_cuda or not points.is_contiguous():
+        raise ValueError("points must be a contiguous CUDA tensor")
+    if n is None:
+        n = _num_records(points, layout)
+    if world_bounds is None and (want_bounds or layout.explicit_dim):
+        world_bounds = torch.empty((2, layout.num_dims), dtype=_bounds_dtype(layout),
+                                   device=points.device)
+    b = BUILDERS[builder] if isinstance(builder, str) else int(builder)
+    _check(lib().cukd_build_tree(_ptr(points), n, C.byref(layout), _ptr(world_bounds), b,
+                                 _stream(stream), None), "cukd_build_tree")
+    return world_bounds
+
+
+def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True,
+            heap_order=False, force_heap=False, block_size=0):
+    p = QueryParams()
+    p.method = METHODS[method] if isinstance(method, str) else int(method)
+    p.k = k
+    p.cutoff_radius = cutoff
+    p.eps = eps
+    p.cutoff_d2 = cutoff_d2
+    p.flags = ((QUERY_MORTON if morton else 0) | (QUERY_HEAP_ORDER if heap_order else 0)
+               | (QUERY_FORCE_HEAP if force_heap else 0))
+    p.block_size = block_size
+    return p
+
+
+def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=None,
+        cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True, with_d2=False,
+        stream=None, block_size=0):
+    """Find-closest-point for each query ([nq, D] tensor of the tree's scalar
+    type).  Returns int32 node indices (-1 = none within the cut-off)."""
+    layout = layout or infer_layout(tree)
+    if n is None:
+        n = _num_records(tree, layout)
+    nq = queries.shape[0]
+    ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
+    d2 = None
+    if with_d2:
+        d2 = torch.empty(nq, dtype=torch.float32 if layout.scalar_type == FLOAT32
+                         else torch.int64, device=queries.device)
+    p = _params(method, 1, cutoff, eps, cutoff_d2, morton, block_size=block_size)
+    _check(lib().cukd_fcp(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                          _ptr(queries.contiguous()), nq, C.byref(p), _ptr(ids), _ptr(d2),
+                          _stream(stream), None), "cukd_fcp")
+    return (ids, d2) if with_d2 else ids
+
+
+def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
+        cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, heap_order=False,
+        force_heap=False, with_max=False, stream=None, block_size=0):
+    """k nearest neighbours.  Returns (ids [nq,k] int32, d2 [nq,k]) with the
+    reference's candidate-list semantics; ascending unless heap_order."""
+    layout = layout or infer_layout(tree)
+    if n is None:
+        n = _num_records(tree, layout)
+    nq = queries.shape[0]
+    dev = queries.device
+    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    dt = torch.float32 if layout.scalar_type == FLOAT32 else torch.int64
+    d2 = torch.empty((nq, k), dtype=dt, device=dev)
+    mx = torch.empty(nq, dtype=dt, device=dev) if with_max else None
+    p = _params(method, k, cutoff, 0.0, cutoff_d2, morton, heap_order, force_heap, block_size)
+    _check(lib().cukd_knn(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                          _ptr(queries.contiguous()), nq, C.byref(p), _ptr(ids), _ptr(d2),
+                          _ptr(mx), _stream(stream), None), "cukd_knn")
+    return (ids, d2, mx) if with_max else (ids, d2)
+
+
+def knn_visits(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
+               cutoff=math.inf, morton=True, stream=None):
+    """Per-query visited-node counts (k=0: FCP traversal)."""
+    layout = layout or infer_layout(tree)
+    if n is None:
+        n = _num_records(tree, layout)
+    nq = queries.shape[0]
+    v = torch.empty(nq, dtype=torch.int64, device=queries.device)
+    p = _params(method, k, cutoff, 0.0, INT64_MAX, morton)
+    _check(lib().cukd_knn_visits(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                                 _ptr(queries.contiguous()), nq, C.byref(p), _ptr(v),
+                                 _stream(stream), None), "cukd_knn_visits")
+    return v
+
+
+def morton_order(points, bounds=None, stream=None):
+    n, D = points.shape
+    perm = torch.empty(n, dtype=torch.int32, device=points.device)
+    _check(lib().cukd_morton_order(_ptr(points.contiguous()), n, D, _ptr(bounds), _ptr(perm),
+                                   _stream(stream), None), "cukd_morton_order")
+    return perm

@@ -1,0 +1,1150 @@
+// Left-balanced k-d tree builder for sm_100a.
+//
+// The reference (cukd/builder_thrust.h:414-512) runs, for every tree level,
+// a full stable sort of (subtree tag, split coordinate) over all N points
+// and then retags (:222-235, :321-345).  Because every sort is stable, the
+// points of the subtree under node g (level l) are ordered by the
+// composite key
+//     (c[dim(g)], c[dim(parent)], c[dim(grandparent)], ..., input index)
+// (a dim already listed is skipped), and the point of rank leftSize(g)
+// (helpers.h:237-252) becomes node g.  This builder computes the same tree
+// by SELECTION on that composite key instead of L full sorts:
+//
+//  global phase -- levels whose subtrees hold more than kTile points; all
+//  subtrees of a level are processed by the same launches:
+//    hist_kernel      histogram of the split coordinate into equal-width
+//                     bins over the subtree's data range
+//    select_kernel    the bin holding rank leftSize(g) (one warp/subtree)
+//    partition_kernel points of lower bins -> left child's segment, higher
+//                     bins -> right child's segment, the pivot bin's points
+//                     -> candidate buffer; grows the children's data bounds
+//    resolve_kernel   MSD radix select over the composite key among the
+//                     candidates; settles the pivot, appends the other
+//                     candidates to the children, derives the children's
+//                     domain boxes and split dims (widest extent of the
+//                     domain box, box.h:112-125, builder_thrust.h:238-306)
+//  subtree phase -- one CTA per subtree of <= kTile points, all remaining
+//    levels in shared memory: one index list per dimension is sorted once
+//    by coordinate; per level the pivot is read from the list of the
+//    level's dim at rank leftSize (an equal-coordinate run around it is
+//    ranked by the composite key), and all lists are stably partitioned
+//    with block-wide scans.
+//  finalize_kernel -- gathers the caller's records into node order and
+//    writes the explicit split dims.
+//
+// Working data are SoA: one uint32 order-preserving key array per
+// dimension plus the input index, ping-ponged between two buffers.
+#include <algorithm>
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace ckb {
+
+static thread_local cudaError_t g_last_cuda = cudaSuccess;
+void set_cuda_error(cudaError_t e) { g_last_cuda = e; }
+const char *last_cuda_error_string() { return cudaGetErrorString(g_last_cuda); }
+
+namespace build {
+
+constexpr int kTile = 2048;       // max subtree size finished in shared memory
+constexpr int kSubThreads = 256;  // threads of the subtree CTA
+constexpr int kChunk = 4096;      // points per CTA in hist / partition
+constexpr int kGThreads = 256;
+constexpr int kMaxBins = 4096;
+
+struct Bufs {
+  uint32_t *key[2][4];
+  uint32_t *idx[2];
+  uint32_t *ckey[4];
+  uint32_t *cidx;
+  uint32_t *perm;  // node -> input index
+  uint8_t *ndim;   // node -> split dim
+  // per-segment arrays: [0] current level, [1] next level
+  uint8_t *sdim[2];
+  uint32_t *sbmin[2], *sbmax[2];  // data bounds as keys, [seg][D]
+  uint32_t *sbox[2];              // domain box as keys, [seg][2D] (lo then hi)
+  uint32_t *hist;                 // [seg][nb]
+  uint32_t *sel;                  // [seg][3]: pivot bin, count below, pivot-bin count
+  uint32_t *cur;                  // [seg][3]: left / right / candidate cursors
+  uint32_t *wbmin, *wbmax;        // world bounds as keys, [D]
+};
+
+// ---------------------------------------------------------------------------
+// scalar helpers
+// ---------------------------------------------------------------------------
+template <int SC> struct Scalar;
+template <> struct Scalar<0> {
+  __device__ static uint32_t key(uint32_t bits) { return float_key(__uint_as_float(bits)); }
+  __device__ static uint32_t bits(uint32_t key) { return __float_as_uint(key_float(key)); }
+  // box.h:112-125 widestDimension (ties to the higher dim) on a key box
+  __device__ static int widest(const uint32_t *lo, const uint32_t *hi, int D)
+  {
+    int best = 0;
+    float wbest = 0.f;
+    for (int d = 0; d < D; d++) {
+      float w = __fsub_rn(key_float(hi[d]), key_float(lo[d]));
+      if (w < wbest) continue;
+      wbest = w;
+      best = d;
+    }
+    return best;
+  }
+};
+template <> struct Scalar<1> {
+  __device__ static uint32_t key(uint32_t bits) { return int_key(int32_t(bits)); }
+  __device__ static uint32_t bits(uint32_t key) { return uint32_t(key_int(key)); }
+  __device__ static int widest(const uint32_t *lo, const uint32_t *hi, int D)
+  {
+    int best = 0;
+    int32_t wbest = 0;
+    for (int d = 0; d < D; d++) {
+      int32_t w = int32_t(uint32_t(key_int(hi[d])) - uint32_t(key_int(lo[d])));
+      if (w < wbest) continue;
+      wbest = w;
+      best = d;
+    }
+    return best;
+  }
+};
+
+// Equal-width binning over a subtree's data range.  Monotone
+// non-decreasing in the key, so composite-key order implies bin order.
+template <int SC> struct Binner;
+template <> struct Binner<0> {
+  float lo, scale;
+  int nb;
+  __device__ Binner(uint32_t klo, uint32_t khi, int nbins) : nb(nbins)
+  {
+    lo = key_float(klo);
+    float span = __fsub_rn(key_float(khi), lo);
+    scale = span > 0.f ? __fdiv_rn(float(nbins), span) : 0.f;
+  }
+  __device__ int operator()(uint32_t k) const
+  {
+    float x = __fmul_rn(__fsub_rn(key_float(k), lo), scale);
+    return x >= 0.f ? (x < float(nb) ? int(x) : nb - 1) : 0;
+  }
+};
+template <> struct Binner<1> {
+  uint32_t klo;
+  uint64_t span;
+  int nb;
+  __device__ Binner(uint32_t lo, uint32_t hi, int nbins) : klo(lo), nb(nbins)
+  {
+    span = hi >= lo ? uint64_t(hi - lo) + 1 : 1;
+  }
+  __device__ int operator()(uint32_t k) const
+  {
+    uint32_t off = k >= klo ? k - klo : 0;
+    uint64_t b = (uint64_t(off) * uint64_t(nb)) / span;
+    return b < uint64_t(nb) ? int(b) : nb - 1;
+  }
+};
+
+__device__ inline int rr_dim(int64_t g, int D) { return level_of(g) % D; }
+
+// ---------------------------------------------------------------------------
+// extract: records -> SoA keys + input index, copy of the records, bounds
+// ---------------------------------------------------------------------------
+template <int SC, int D>
+__global__ void __launch_bounds__(256) extract_kernel(const uint8_t *__restrict__ pts, int64_t n,
+                                                      int stride, int poff,
+                                                      uint8_t *__restrict__ orig, Bufs b)
+{
+  uint32_t lo[D], hi[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    lo[d] = 0xffffffffu;
+    hi[d] = 0u;
+  }
+  const int words = stride >> 2;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const uint32_t *src = (const uint32_t *)(pts + i * stride);
+    uint32_t *dst = (uint32_t *)(orig + i * stride);
+    for (int w = 0; w < words; w++) dst[w] = src[w];
+    const uint32_t *c = (const uint32_t *)(pts + i * stride + poff);
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      uint32_t k = Scalar<SC>::key(c[d]);
+      b.key[0][d][i] = k;
+      lo[d] = min(lo[d], k);
+      hi[d] = max(hi[d], k);
+    }
+    b.idx[0][i] = uint32_t(i);
+  }
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = min(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = max(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+    if ((threadIdx.x & 31) == 0 && lo[d] <= hi[d]) {
+      atomicMin(&b.wbmin[d], lo[d]);
+      atomicMax(&b.wbmax[d], hi[d]);
+    }
+  }
+}
+
+// root subtree info and the optional world-bounds output (box_t layout)
+template <int SC, int D>
+__global__ void root_kernel(Bufs b, void *worldBounds, bool explicitDims)
+{
+  if (threadIdx.x != 0) return;
+  uint32_t *wb = (uint32_t *)worldBounds;
+  for (int d = 0; d < D; d++) {
+    if (wb) {
+      wb[d] = Scalar<SC>::bits(b.wbmin[d]);
+      wb[D + d] = Scalar<SC>::bits(b.wbmax[d]);
+    }
+    b.sbmin[0][d] = b.wbmin[d];
+    b.sbmax[0][d] = b.wbmax[d];
+    b.sbox[0][d] = b.wbmin[d];
+    b.sbox[0][D + d] = b.wbmax[d];
+  }
+  b.sdim[0][0] = explicitDims ? uint8_t(Scalar<SC>::widest(b.wbmin, b.wbmax, D)) : 0;
+}
+
+// ---------------------------------------------------------------------------
+// global phase kernels
+// ---------------------------------------------------------------------------
+struct LevelArgs {
+  int64_t n;
+  int level;
+  int nb;
+  int chunksPerSeg;
+  int nseg;
+  int cb;  // current key buffer
+};
+
+template <int SC, int D>
+__global__ void __launch_bounds__(kGThreads) hist_kernel(Bufs b, LevelArgs a)
+{
+  __shared__ uint32_t sh[kMaxBins];
+  const int seg = blockIdx.x / a.chunksPerSeg;
+  const int chunk = blockIdx.x % a.chunksPerSeg;
+  const int64_t g = ((int64_t(1) << a.level) - 1) + seg;
+  const int64_t sb = seg_begin(g, a.level, a.n);
+  const int64_t sz = subtree_size(g, a.n);
+  const int64_t c0 = int64_t(chunk) * kChunk;
+  if (c0 >= sz) return;
+  const int64_t c1 = min(sz, c0 + kChunk);
+  for (int i = threadIdx.x; i < a.nb; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const int dim = b.sdim[0][seg];
+  const Binner<SC> bin(b.sbmin[0][seg * D + dim], b.sbmax[0][seg * D + dim], a.nb);
+  const uint32_t *__restrict__ kd = b.key[a.cb][dim] + sb;
+  for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) atomicAdd(&sh[bin(kd[i])], 1u);
+  __syncthreads();
+  uint32_t *gh = b.hist + int64_t(seg) * a.nb;
+  for (int i = threadIdx.x; i < a.nb; i += blockDim.x)
+    if (sh[i]) atomicAdd(&gh[i], sh[i]);
+}
+
+// one warp per subtree: the bin that holds rank leftSize(g)
+__global__ void select_kernel(Bufs b, LevelArgs a)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= a.nseg) return;
+  const int64_t g = ((int64_t(1) << a.level) - 1) + warp;
+  const uint32_t r = uint32_t(left_size(g, a.n));
+  const uint32_t *h = b.hist + int64_t(warp) * a.nb;
+  const int per = a.nb / 32;
+  uint32_t s = 0;
+  for (int i = 0; i < per; i++) s += h[lane * per + i];
+  uint32_t incl = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const uint32_t excl = incl - s;
+  if (r >= excl && r < incl) {
+    uint32_t cum = excl;
+    for (int i = 0; i < per; i++) {
+      uint32_t c = h[lane * per + i];
+      if (r < cum + c) {
+        b.sel[warp * 3 + 0] = uint32_t(lane * per + i);
+        b.sel[warp * 3 + 1] = cum;
+        b.sel[warp * 3 + 2] = c;
+        break;
+      }
+      cum += c;
+    }
+  }
+  if (lane < 3) b.cur[warp * 3 + lane] = 0;
+}
+
+// warp-reduce per-child bounds and merge them into the next level's arrays
+template <int D>
+__device__ inline void merge_child_bounds(uint32_t (&lo)[2][D], uint32_t (&hi)[2][D],
+                                          uint32_t *bmin, uint32_t *bmax, int64_t childIdx)
+{
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      uint32_t l = lo[s][d], h = hi[s][d];
+      for (int o = 16; o > 0; o >>= 1) {
+        l = min(l, __shfl_xor_sync(0xffffffffu, l, o));
+        h = max(h, __shfl_xor_sync(0xffffffffu, h, o));
+      }
+      if ((threadIdx.x & 31) == 0 && l <= h) {
+        atomicMin(&bmin[(childIdx + s) * D + d], l);
+        atomicMax(&bmax[(childIdx + s) * D + d], h);
+      }
+    }
+}
+
+template <int SC, int D>
+__global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs a)
+{
+  constexpr int PER = kChunk / kGThreads;
+  static_assert(PER <= 16, "2-bit class codes packed in one uint32");
+  __shared__ uint32_t warpTot[kGThreads / 32][3];
+  __shared__ uint32_t base[3];
+  const int seg = blockIdx.x / a.chunksPerSeg;
+  const int chunk = blockIdx.x % a.chunksPerSeg;
+  const int64_t g = ((int64_t(1) << a.level) - 1) + seg;
+  const int64_t sb = seg_begin(g, a.level, a.n);
+  const int64_t sz = subtree_size(g, a.n);
+  const int64_t c0 = int64_t(chunk) * kChunk;
+  if (c0 >= sz) return;
+  const int64_t c1 = min(sz, c0 + kChunk);
+  const int dim = b.sdim[0][seg];
+  const Binner<SC> bin(b.sbmin[0][seg * D + dim], b.sbmax[0][seg * D + dim], a.nb);
+  const uint32_t pb = b.sel[seg * 3 + 0];
+  const int cb = a.cb, nbuf = cb ^ 1;
+  const uint32_t *__restrict__ kd = b.key[cb][dim] + sb;
+
+  // pass 1: class 0 = left, 1 = right, 2 = candidate
+  uint32_t cls = 0;
+  uint32_t cnt[3] = {0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const int64_t i = c0 + threadIdx.x + int64_t(j) * kGThreads;
+    if (i < c1) {
+      const uint32_t bb = uint32_t(bin(kd[i]));
+      const uint32_t c = bb < pb ? 0u : (bb > pb ? 1u : 2u);
+      cls |= c << (2 * j);
+      cnt[c]++;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t excl[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    uint32_t v = cnt[c];
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    excl[c] = v - cnt[c];
+    if (lane == 31) warpTot[wid][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int c = threadIdx.x;
+    uint32_t tot = 0;
+    for (int w = 0; w < kGThreads / 32; w++) {
+      uint32_t t = warpTot[w][c];
+      warpTot[w][c] = tot;
+      tot += t;
+    }
+    base[c] = tot ? atomicAdd(&b.cur[seg * 3 + c], tot) : 0u;
+  }
+  __syncthreads();
+  uint32_t pos[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) pos[c] = base[c] + warpTot[wid][c] + excl[c];
+
+  const int64_t lchild = 2 * g + 1;
+  const int lvlNext = a.level + 1;
+  const int64_t lBeg = seg_begin(lchild, lvlNext, a.n);
+  const int64_t rBeg = seg_begin(lchild + 1, lvlNext, a.n);
+  uint32_t lo[2][D], hi[2][D];
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      lo[s][d] = 0xffffffffu;
+      hi[s][d] = 0u;
+    }
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const int64_t i = c0 + threadIdx.x + int64_t(j) * kGThreads;
+    if (i < c1) {
+      const uint32_t c = (cls >> (2 * j)) & 3u;
+      uint32_t k[D];
+#pragma unroll
+      for (int d = 0; d < D; d++) k[d] = b.key[cb][d][sb + i];
+      const uint32_t id = b.idx[cb][sb + i];
+      if (c == 2) {
+        const int64_t dst = sb + pos[2]++;
+#pragma unroll
+        for (int d = 0; d < D; d++) b.ckey[d][dst] = k[d];
+        b.cidx[dst] = id;
+      } else {
+        const int64_t dst = (c == 0 ? lBeg : rBeg) + pos[c]++;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          b.key[nbuf][d][dst] = k[d];
+          lo[c][d] = min(lo[c][d], k[d]);
+          hi[c][d] = max(hi[c][d], k[d]);
+        }
+        b.idx[nbuf][dst] = id;
+      }
+    }
+  }
+  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], 2 * int64_t(seg));
+}
+
+// MSD radix select on the composite key among a subtree's candidates, then
+// the candidates' final placement.  One CTA per subtree.
+template <int SC, int D>
+__global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
+                                                            bool explicitDims)
+{
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr;
+  __shared__ uint32_t pw[D + 1];
+  const int seg = blockIdx.x;
+  const int64_t g = ((int64_t(1) << a.level) - 1) + seg;
+  const int64_t sb = seg_begin(g, a.level, a.n);
+  const int64_t sz = subtree_size(g, a.n);
+  const uint32_t below = b.sel[seg * 3 + 1];
+  const uint32_t m = b.sel[seg * 3 + 2];
+  const uint32_t r = uint32_t(left_size(g, a.n));
+  const int dim = b.sdim[0][seg];
+
+  // composite order: own dim, then ancestors' dims nearest first, then index
+  int cd[D];
+  int ncd = 0;
+  cd[ncd++] = dim;
+  for (int64_t an = g; an > 0 && ncd < D;) {
+    an = (an - 1) >> 1;
+    const int da = explicitDims ? int(b.ndim[an]) : rr_dim(an, D);
+    bool seen = false;
+    for (int i = 0; i < ncd; i++) seen |= (cd[i] == da);
+    if (!seen) cd[ncd++] = da;
+  }
+  const int nwords = ncd + 1;
+  auto word = [&](uint32_t i, int w) -> uint32_t {
+    return w < ncd ? b.ckey[cd[w]][sb + i] : b.cidx[sb + i];
+  };
+
+  uint32_t rank = r - below;
+  bool unique = false;
+  int w = 0;
+  uint32_t cp = 0, cm = 0;
+  for (w = 0; w < nwords && !unique; w++) {
+    cp = 0;
+    cm = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+        bool ok = true;
+        for (int pw_i = 0; pw_i < w && ok; pw_i++) ok = word(i, pw_i) == pw[pw_i];
+        if (!ok) continue;
+        const uint32_t v = word(i, w);
+        if ((v & cm) != cp) continue;
+        atomicAdd(&hist[(v >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        uint32_t s = 0;
+        for (int k = 0; k < 8; k++) s += hist[lane * 8 + k];
+        uint32_t incl = s;
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const uint32_t excl = incl - s;
+        if (rank >= excl && rank < incl) {
+          uint32_t cum = excl;
+          for (int k = 0; k < 8; k++) {
+            const uint32_t c = hist[lane * 8 + k];
+            if (rank < cum + c) {
+              sDigit = uint32_t(lane * 8 + k);
+              sCount = c;
+              sRank = rank - cum;
+              break;
+            }
+            cum += c;
+          }
+        }
+      }
+      __syncthreads();
+      rank = sRank;
+      cp |= sDigit << shift;
+      cm |= 0xffu << shift;
+      if (sCount == 1) {
+        unique = true;
+        break;
+      }
+    }
+    if (!unique && threadIdx.x == 0) pw[w] = cp;
+    __syncthreads();
+  }
+  // w now indexes the word being matched when the pivot became unique
+  // (or nwords when every word was fully resolved; the index is unique).
+  const int wl = unique ? w - 1 : nwords - 1;
+  if (!unique) {
+    cp = pw[nwords - 1];
+    cm = 0xffffffffu;
+  }
+  if (threadIdx.x == 0) sPivot = 0xffffffffu;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+    bool ok = true;
+    for (int pw_i = 0; pw_i < wl && ok; pw_i++) ok = word(i, pw_i) == pw[pw_i];
+    if (ok && (word(i, wl) & cm) == cp) sPivot = i;
+  }
+  if (threadIdx.x == 0) {
+    sNl = 0;
+    sNr = 0;
+  }
+  __syncthreads();
+  // exactly one candidate matches; the clamp only guards memory safety
+  const uint32_t piv = sPivot < m ? sPivot : 0u;
+  uint32_t pk[D + 1];
+  for (int x = 0; x < nwords; x++) pk[x] = word(piv, x);
+  uint32_t pkey[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) pkey[d] = b.ckey[d][sb + piv];
+
+  const int64_t lchild = 2 * g + 1;
+  const int lvlNext = a.level + 1;
+  const int64_t lBeg = seg_begin(lchild, lvlNext, a.n) + below;
+  const int64_t rBeg = seg_begin(lchild + 1, lvlNext, a.n) + (uint32_t(sz) - m - below);
+  const int nbuf = a.cb ^ 1;
+  uint32_t lo[2][D], hi[2][D];
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      lo[s][d] = 0xffffffffu;
+      hi[s][d] = 0u;
+    }
+  for (uint32_t i0 = 0; i0 < m; i0 += blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    if (i < m && i != piv) {
+      int side = 0;  // 0 left, 1 right
+      for (int x = 0; x < nwords; x++) {
+        const uint32_t v = word(i, x);
+        if (v != pk[x]) {
+          side = v > pk[x];
+          break;
+        }
+      }
+      const int64_t dst = side ? rBeg + atomicAdd(&sNr, 1u) : lBeg + atomicAdd(&sNl, 1u);
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const uint32_t k = b.ckey[d][sb + i];
+        b.key[nbuf][d][dst] = k;
+        lo[side][d] = min(lo[side][d], k);
+        hi[side][d] = max(hi[side][d], k);
+      }
+      b.idx[nbuf][dst] = b.cidx[sb + i];
+    }
+  }
+  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], 2 * int64_t(seg));
+  if (threadIdx.x == 0) {
+    b.perm[g] = b.cidx[sb + piv];
+    b.ndim[g] = uint8_t(dim);
+    uint32_t bl[D], bh[D];
+    for (int d = 0; d < D; d++) {
+      bl[d] = b.sbox[0][int64_t(seg) * 2 * D + d];
+      bh[d] = b.sbox[0][int64_t(seg) * 2 * D + D + d];
+    }
+    for (int s = 0; s < 2; s++) {
+      uint32_t cl[D], ch[D];
+      for (int d = 0; d < D; d++) {
+        cl[d] = bl[d];
+        ch[d] = bh[d];
+      }
+      if (s == 0)
+        ch[dim] = pkey[dim];
+      else
+        cl[dim] = pkey[dim];
+      const int64_t ci = 2 * int64_t(seg) + s;
+      for (int d = 0; d < D; d++) {
+        b.sbox[1][ci * 2 * D + d] = cl[d];
+        b.sbox[1][ci * 2 * D + D + d] = ch[d];
+      }
+      b.sdim[1][ci] = explicitDims ? uint8_t(Scalar<SC>::widest(cl, ch, D))
+                                   : uint8_t((a.level + 1) % D);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// subtree phase: one CTA per subtree of <= kTile points
+// ---------------------------------------------------------------------------
+template <int D>
+struct SubSmem {
+  uint32_t key[D][kTile];
+  uint32_t idx[kTile];
+  uint16_t list[2][D][kTile];
+  uint16_t segOf[2][kTile];
+  uint32_t scan[kTile];
+  union {
+    unsigned long long sortbuf[kTile];
+    struct {
+      uint16_t t0[kTile], t1[kTile], b[kTile], r[kTile];
+    } sub;
+  } u;
+  uint16_t locPivot[2 * kTile];
+  uint8_t locDim[2 * kTile];
+  uint8_t flag[kTile];
+  uint8_t subDim[kTile];
+  uint16_t queue[kTile];
+  uint32_t warpSums[kSubThreads / 32];
+  uint32_t qcount;
+  uint32_t rootLo[D], rootHi[D];
+};
+
+template <int SC, int D>
+__global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
+                                                              bool explicitDims)
+{
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  SubSmem<D> &S = *reinterpret_cast<SubSmem<D> *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int seg = blockIdx.x;
+  const int64_t s = ((int64_t(1) << L0) - 1) + seg;
+  const int64_t sb = seg_begin(s, L0, n);
+  const int m = int(subtree_size(s, n));
+  if (m == 0) return;
+
+  for (int i = tid; i < m; i += kSubThreads) {
+#pragma unroll
+    for (int d = 0; d < D; d++) S.key[d][i] = b.key[cb][d][sb + i];
+    S.idx[i] = b.idx[cb][sb + i];
+    S.segOf[0][i] = 0;
+  }
+  if (tid < D) {
+    S.rootLo[tid] = b.sbox[0][int64_t(seg) * 2 * D + tid];
+    S.rootHi[tid] = b.sbox[0][int64_t(seg) * 2 * D + D + tid];
+  }
+  __syncthreads();
+
+  // one coordinate-sorted index list per dimension (bitonic sort of
+  // key << 32 | index; equal keys in any order)
+  int P = 1;
+  while (P < m) P <<= 1;
+  for (int d = 0; d < D; d++) {
+    for (int i = tid; i < P; i += kSubThreads)
+      S.u.sortbuf[i] = i < m ? ((unsigned long long)S.key[d][i] << 32) | uint32_t(i)
+                             : ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= P; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = tid; i < P; i += kSubThreads) {
+          const int l = i ^ j;
+          if (l > i) {
+            const unsigned long long x = S.u.sortbuf[i], y = S.u.sortbuf[l];
+            const bool up = (i & k) == 0;
+            if ((x > y) == up) {
+              S.u.sortbuf[i] = y;
+              S.u.sortbuf[l] = x;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = tid; i < m; i += kSubThreads) S.list[0][d][i] = uint16_t(S.u.sortbuf[i]);
+    __syncthreads();
+  }
+
+  int cur = 0;
+  int mact = m;
+  const int lane = tid & 31, wid = tid >> 5;
+  for (int j = 0; mact > 0; j++) {
+    const int lvl = L0 + j;
+    const int64_t g0 = ((s + 1) << j) - 1;
+    const int64_t base0 = seg_begin(g0, lvl, n);
+    const int nsub = 1 << j;
+    int nexist = int(min(int64_t(nsub), max(int64_t(0), n - g0)));
+    if (tid == 0) S.qcount = 0;
+    __syncthreads();
+    // A: per subtree, its dim, pivot rank position and equal-key run
+    for (int t = tid; t < nexist; t += kSubThreads) {
+      const int64_t g = g0 + t;
+      const int sz = int(subtree_size(g, n));
+      const int bt = int(seg_begin(g, lvl, n) - base0);
+      const int r = int(left_size(g, n));
+      const int u = (1 << j) - 1 + t;
+      int dim;
+      if (explicitDims) {
+        uint32_t lo[D], hi[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          lo[d] = S.rootLo[d];
+          hi[d] = S.rootHi[d];
+        }
+        for (int c = u; c > 0;) {
+          const int p = (c - 1) >> 1;
+          const int pd = S.locDim[p];
+          const uint32_t pc = S.key[pd][S.locPivot[p]];
+          if (c & 1)
+            hi[pd] = min(hi[pd], pc);
+          else
+            lo[pd] = max(lo[pd], pc);
+          c = p;
+        }
+        dim = Scalar<SC>::widest(lo, hi, D);
+      } else {
+        dim = lvl % D;
+      }
+      S.locDim[u] = uint8_t(dim);
+      const uint16_t *Ld = S.list[cur][dim];
+      const uint32_t *Kd = S.key[dim];
+      const int pp = bt + r;
+      const uint32_t v = Kd[Ld[pp]];
+      int lo = bt, hi = pp;  // first q in [bt,pp] with key >= v
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (Kd[Ld[mid]] < v)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      const int t0 = lo;
+      lo = pp + 1;
+      hi = bt + sz;  // first q in [pp+1, bt+sz) with key > v
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (Kd[Ld[mid]] <= v)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      const int t1 = lo;
+      S.u.sub.t0[t] = uint16_t(t0);
+      S.u.sub.t1[t] = uint16_t(t1);
+      S.u.sub.b[t] = uint16_t(bt);
+      S.u.sub.r[t] = uint16_t(r);
+      S.subDim[t] = uint8_t(dim);
+      if (t1 - t0 == 1) {
+        const int piv = Ld[pp];
+        S.flag[piv] = 2;
+        S.locPivot[u] = uint16_t(piv);
+        b.perm[g] = S.idx[piv];
+        b.ndim[g] = uint8_t(dim);
+      } else {
+        S.queue[atomicAdd(&S.qcount, 1u)] = uint16_t(t);
+      }
+    }
+    __syncthreads();
+    // A2: rank equal-coordinate runs by the composite key (one warp each)
+    for (int qi = wid; qi < int(S.qcount); qi += kSubThreads / 32) {
+      const int t = S.queue[qi];
+      const int64_t g = g0 + t;
+      const int u = (1 << j) - 1 + t;
+      const int dim = S.subDim[t];
+      const int t0 = S.u.sub.t0[t], t1 = S.u.sub.t1[t];
+      const int pp = S.u.sub.b[t] + S.u.sub.r[t];
+      int cd[D];
+      int ncd = 0;
+      cd[ncd++] = dim;
+      {
+        int c = u;
+        int64_t ga = g;
+        while (ga > 0 && ncd < D) {
+          int da;
+          if (c > 0) {
+            c = (c - 1) >> 1;
+            da = S.locDim[c];
+          } else {
+            da = explicitDims ? int(b.ndim[(ga - 1) >> 1]) : rr_dim((ga - 1) >> 1, D);
+          }
+          ga = (ga - 1) >> 1;
+          bool seen = false;
+          for (int i = 0; i < ncd; i++) seen |= (cd[i] == da);
+          if (!seen) cd[ncd++] = da;
+        }
+      }
+      const uint16_t *Ld = S.list[cur][dim];
+      const int len = t1 - t0;
+      for (int x = lane; x < len; x += 32) {
+        const int ex = Ld[t0 + x];
+        int rk = 0;
+        for (int y = 0; y < len; y++) {
+          const int ey = Ld[t0 + y];
+          bool less = false, decided = false;
+          for (int w = 1; w < ncd && !decided; w++) {
+            const uint32_t ky = S.key[cd[w]][ey], kx = S.key[cd[w]][ex];
+            if (ky != kx) {
+              less = ky < kx;
+              decided = true;
+            }
+          }
+          if (!decided) less = S.idx[ey] < S.idx[ex];
+          rk += less;
+        }
+        const int want = pp - t0;
+        if (rk < want)
+          S.flag[ex] = 0;
+        else if (rk > want)
+          S.flag[ex] = 1;
+        else {
+          S.flag[ex] = 2;
+          S.locPivot[u] = uint16_t(ex);
+          b.perm[g] = S.idx[ex];
+          b.ndim[g] = uint8_t(dim);
+        }
+      }
+    }
+    __syncthreads();
+    // B: sides of all points outside the runs
+    for (int p = tid; p < mact; p += kSubThreads) {
+      const int t = S.segOf[cur][p];
+      const int e = S.list[cur][S.subDim[t]][p];
+      if (p < S.u.sub.t0[t])
+        S.flag[e] = 0;
+      else if (p >= S.u.sub.t1[t])
+        S.flag[e] = 1;
+    }
+    __syncthreads();
+    // C: stable partition of every list (pivots dropped)
+    constexpr int PER = kTile / kSubThreads;
+    for (int d = 0; d < D; d++) {
+      const uint16_t *Lc = S.list[cur][d];
+      uint32_t local = 0;
+      const int p0 = tid * PER;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int p = p0 + q;
+        if (p < mact) {
+          const int f = S.flag[Lc[p]];
+          local += f == 0 ? 1u : (f == 1 ? 0x10000u : 0u);
+        }
+      }
+      uint32_t incl = local;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) S.warpSums[wid] = incl;
+      __syncthreads();
+      uint32_t wbase = 0;
+      for (int w = 0; w < wid; w++) wbase += S.warpSums[w];
+      uint32_t run = wbase + incl - local;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int p = p0 + q;
+        if (p < mact) {
+          S.scan[p] = run;
+          const int f = S.flag[Lc[p]];
+          run += f == 0 ? 1u : (f == 1 ? 0x10000u : 0u);
+        }
+      }
+      __syncthreads();
+      for (int p = tid; p < mact; p += kSubThreads) {
+        const int e = Lc[p];
+        const int f = S.flag[e];
+        if (f == 2) continue;
+        const int t = S.segOf[cur][p];
+        const int bt = S.u.sub.b[t];
+        const uint32_t sbase = S.scan[bt], sp = S.scan[p];
+        const int nb = bt - t;
+        const int np = f == 0 ? nb + int((sp & 0xffffu) - (sbase & 0xffffu))
+                              : nb + S.u.sub.r[t] + int((sp >> 16) - (sbase >> 16));
+        S.list[cur ^ 1][d][np] = uint16_t(e);
+        if (d == 0) S.segOf[cur ^ 1][np] = uint16_t(2 * t + f);
+      }
+      __syncthreads();
+    }
+    mact -= nexist;
+    cur ^= 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// finalize: records in node order (+ explicit dims)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) finalize_kernel(uint8_t *__restrict__ pts,
+                                                       const uint8_t *__restrict__ orig,
+                                                       const uint32_t *__restrict__ perm,
+                                                       const uint8_t *__restrict__ ndim,
+                                                       int64_t n, int stride, int doff,
+                                                       int dshift, uint32_t dmask)
+{
+  const int words = stride >> 2;
+  for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < n;
+       g += int64_t(gridDim.x) * blockDim.x) {
+    uint32_t pi = perm[g];
+    if (pi >= uint64_t(n)) pi = uint32_t(g);  // guards memory safety only
+    const uint32_t *src = (const uint32_t *)(orig + int64_t(pi) * stride);
+    uint32_t *dst = (uint32_t *)(pts + g * stride);
+    for (int w = 0; w < words; w++) dst[w] = src[w];
+    if (doff >= 0) {
+      uint32_t *dw = (uint32_t *)(pts + g * stride + doff);
+      *dw = (*dw & ~(dmask << dshift)) | ((uint32_t(ndim[g]) & dmask) << dshift);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+static int pow2ceil(int64_t v)
+{
+  int p = 1;
+  while (p < v && p < (1 << 30)) p <<= 1;
+  return p;
+}
+
+template <int SC, int D>
+int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st,
+               const cukd_mem_resource *mem)
+{
+  const bool explicitDims = L.doff >= 0;
+  TempArena arena(st, mem);
+  Bufs b = {};
+  int G = 0;
+  while (subtree_size((int64_t(1) << G) - 1, n) > kTile) G++;
+  const int64_t capSeg = int64_t(1) << G;
+  for (int x = 0; x < 2; x++) {
+    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.key[x][d], n));
+    CKB_TRY(arena.alloc(&b.idx[x], n));
+  }
+  if (G > 0) {
+    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.ckey[d], n));
+    CKB_TRY(arena.alloc(&b.cidx, n));
+  }
+  CKB_TRY(arena.alloc(&b.perm, n));
+  CKB_TRY(arena.alloc(&b.ndim, n));
+  uint8_t *orig = nullptr;
+  CKB_TRY(arena.alloc(&orig, size_t(n) * L.stride));
+  for (int x = 0; x < 2; x++) {
+    CKB_TRY(arena.alloc(&b.sdim[x], capSeg));
+    CKB_TRY(arena.alloc(&b.sbmin[x], capSeg * D));
+    CKB_TRY(arena.alloc(&b.sbmax[x], capSeg * D));
+    CKB_TRY(arena.alloc(&b.sbox[x], capSeg * 2 * D));
+  }
+  int64_t histCap = 64;
+  for (int lvl = 0; lvl < G; lvl++) {
+    const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
+    const int nb = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
+    histCap = std::max(histCap, (int64_t(1) << lvl) * nb);
+  }
+  CKB_TRY(arena.alloc(&b.hist, histCap));
+  CKB_TRY(arena.alloc(&b.sel, capSeg * 3));
+  CKB_TRY(arena.alloc(&b.cur, capSeg * 3));
+  CKB_TRY(arena.alloc(&b.wbmin, D));
+  CKB_TRY(arena.alloc(&b.wbmax, D));
+
+  CKB_CUDA(cudaMemsetAsync(b.perm, 0xff, sizeof(uint32_t) * n, st));
+  CKB_CUDA(cudaMemsetAsync(b.wbmin, 0xff, sizeof(uint32_t) * D, st));
+  CKB_CUDA(cudaMemsetAsync(b.wbmax, 0, sizeof(uint32_t) * D, st));
+  {
+    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 8));
+    extract_kernel<SC, D><<<blocks, 256, 0, st>>>((const uint8_t *)pts, n, L.stride, L.poff,
+                                                  orig, b);
+    CKB_CHECK_LAUNCH();
+  }
+  root_kernel<SC, D><<<1, 32, 0, st>>>(b, worldBounds, explicitDims);
+  CKB_CHECK_LAUNCH();
+
+  int cb = 0;
+  for (int lvl = 0; lvl < G; lvl++) {
+    const int nseg = 1 << lvl;
+    const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
+    LevelArgs a;
+    a.n = n;
+    a.level = lvl;
+    a.nb = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
+    a.chunksPerSeg = int(div_up(maxSeg, kChunk));
+    a.nseg = nseg;
+    a.cb = cb;
+    CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
+    CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * 2 * nseg * D, st));
+    CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * 2 * nseg * D, st));
+    const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
+    hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    partition_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
+    CKB_CHECK_LAUNCH();
+    cb ^= 1;
+    std::swap(b.sdim[0], b.sdim[1]);
+    std::swap(b.sbmin[0], b.sbmin[1]);
+    std::swap(b.sbmax[0], b.sbmax[1]);
+    std::swap(b.sbox[0], b.sbox[1]);
+  }
+  {
+    const size_t smem = sizeof(SubSmem<D>);
+    CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
+                                                                       explicitDims);
+    CKB_CHECK_LAUNCH();
+  }
+  {
+    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 16));
+    finalize_kernel<<<blocks, 256, 0, st>>>((uint8_t *)pts, orig, b.perm, b.ndim, n, L.stride,
+                                            explicitDims ? L.doff : -1, L.dshift, L.dmask);
+    CKB_CHECK_LAUNCH();
+  }
+  return CUKD_OK;
+}
+
+template <int SC, int D>
+__global__ void bounds_only_kernel(const uint8_t *__restrict__ pts, int64_t n, int stride,
+                                   int poff, uint32_t *kmin, uint32_t *kmax)
+{
+  uint32_t lo[D], hi[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    lo[d] = 0xffffffffu;
+    hi[d] = 0u;
+  }
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const uint32_t *c = (const uint32_t *)(pts + i * stride + poff);
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const uint32_t k = Scalar<SC>::key(c[d]);
+      lo[d] = min(lo[d], k);
+      hi[d] = max(hi[d], k);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = min(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = max(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+    if ((threadIdx.x & 31) == 0 && lo[d] <= hi[d]) {
+      atomicMin(&kmin[d], lo[d]);
+      atomicMax(&kmax[d], hi[d]);
+    }
+  }
+}
+
+template <int SC, int D>
+__global__ void bounds_write_kernel(const uint32_t *kmin, const uint32_t *kmax, uint32_t *out)
+{
+  if (threadIdx.x < D) {
+    out[threadIdx.x] = Scalar<SC>::bits(kmin[threadIdx.x]);
+    out[D + threadIdx.x] = Scalar<SC>::bits(kmax[threadIdx.x]);
+  }
+}
+
+template <int SC, int D>
+int bounds_impl(const void *pts, int64_t n, const Layout &L, void *out, cudaStream_t st)
+{
+  TempArena arena(st, nullptr);
+  uint32_t *k = nullptr;
+  CKB_TRY(arena.alloc(&k, 2 * D));
+  CKB_CUDA(cudaMemsetAsync(k, 0xff, sizeof(uint32_t) * D, st));
+  CKB_CUDA(cudaMemsetAsync(k + D, 0, sizeof(uint32_t) * D, st));
+  const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(div_up(n, 256), kNumSMs * 8)));
+  bounds_only_kernel<SC, D><<<blocks, 256, 0, st>>>((const uint8_t *)pts, n, L.stride, L.poff,
+                                                    k, k + D);
+  CKB_CHECK_LAUNCH();
+  bounds_write_kernel<SC, D><<<1, 32, 0, st>>>(k, k + D, (uint32_t *)out);
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+}  // namespace build
+
+int build_dispatch(void *pts, int64_t n, const Layout &L, void *wb, cudaStream_t st,
+                   const cukd_mem_resource *mem)
+{
+  using namespace build;
+#define CKB_CASE(SC_, D_) \
+  if (L.scalar == SC_ && L.D == D_) return build_impl<SC_, D_>(pts, n, L, wb, st, mem);
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
+  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+#undef CKB_CASE
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+int bounds_dispatch(const void *pts, int64_t n, const Layout &L, void *out, cudaStream_t st)
+{
+  using namespace build;
+#define CKB_CASE(SC_, D_) \
+  if (L.scalar == SC_ && L.D == D_) return bounds_impl<SC_, D_>(pts, n, L, out, st);
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
+  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+#undef CKB_CASE
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+}  // namespace ckb
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int cukd_build_tree(void *d_points, int64_t n, const cukd_layout *layout, void *d_world_bounds,
+                    int builder, cudaStream_t stream, const cukd_mem_resource *mem)
+{
+  ckb::Layout L;
+  if (!ckb::make_layout(layout, &L)) return CUKD_ERR_INVALID_ARGUMENT;
+  if (builder < CUKD_BUILDER_DEFAULT || builder > CUKD_BUILDER_INPLACE)
+    return CUKD_ERR_INVALID_ARGUMENT;
+  if (n < 1) return CUKD_OK;
+  if (L.doff >= 0 && !d_world_bounds) return CUKD_ERR_MISSING_WORLD_BOUNDS;
+  if (!d_points) return CUKD_ERR_INVALID_ARGUMENT;
+  if (n > (int64_t(1) << 31) - 1) return CUKD_ERR_UNSUPPORTED;
+  return ckb::build_dispatch(d_points, n, L, d_world_bounds, stream, mem);
+}
+
+int cukd_compute_bounds(const void *d_points, int64_t n, const cukd_layout *layout,
+                        void *d_world_bounds, cudaStream_t stream)
+{
+  ckb::Layout L;
+  if (!ckb::make_layout(layout, &L) || !d_world_bounds) return CUKD_ERR_INVALID_ARGUMENT;
+  if (n < 1) return CUKD_OK;
+  return ckb::bounds_dispatch(d_points, n, L, d_world_bounds, stream);
+}
+
+#define CKB_TYPED(name, SC, D)                                                            \
+  int name(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,          \
+           const cukd_mem_resource *mem)                                                  \
+  {                                                                                       \
+    cukd_layout l = {SC, D, 4 * D, 0, -1, 0, 0};                                          \
+    return cukd_build_tree(d_points, n, &l, d_world_bounds, CUKD_BUILDER_DEFAULT, stream, \
+                           mem);                                                          \
+  }
+CKB_TYPED(cukd_build_float2, CUKD_FLOAT32, 2)
+CKB_TYPED(cukd_build_float3, CUKD_FLOAT32, 3)
+CKB_TYPED(cukd_build_float4, CUKD_FLOAT32, 4)
+CKB_TYPED(cukd_build_int2, CUKD_INT32, 2)
+CKB_TYPED(cukd_build_int3, CUKD_INT32, 3)
+CKB_TYPED(cukd_build_int4, CUKD_INT32, 4)
+#undef CKB_TYPED
+
+const char *cukd_status_string(int status)
+{
+  switch (status) {
+    case CUKD_OK: return "success";
+    case CUKD_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case CUKD_ERR_MISSING_WORLD_BOUNDS:
+      return "asked to build k-d tree over nodes with explicit dims, but no memory for world "
+             "bounds provided";
+    case CUKD_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case CUKD_ERR_CUDA: return "CUDA error";
+    case CUKD_ERR_UNSUPPORTED: return "unsupported data layout or size";
+    case CUKD_ERR_TIMEOUT: return "device-side wait timed out";
+    case CUKD_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+  }
+  return "unknown status";
+}
+
+const char *cukd_last_cuda_error(void) { return ckb::last_cuda_error_string(); }
+
+}  // extern "C"

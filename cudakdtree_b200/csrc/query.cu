@@ -1,0 +1,217 @@
+// Whole-batch FCP / kNN queries over a left-balanced k-d tree (sm_100a).
+//
+// One thread runs one query with exactly the reference's control flow --
+// traverse_default (traverse-default-stack-based.h:24-108),
+// traverse_stack_free (traverse-stack-free.h:24-117) and traverse_cct
+// (traverse-cct.h:25-99) -- so candidates reach the result object in the
+// same order and the answers are bit-identical, ties included.  What is
+// B200-specific is around that core:
+//   - queries are visited in 30-bit Morton order (morton.cu) so a warp's
+//     32 traversals walk nearby paths, and results are scattered back;
+//   - node records are read through the read-only path (__ldg), 16-byte
+//     vector loads for 16-byte records;
+//   - fixed-size candidate lists live in registers with an early-out
+//     before the insertion network (same result: a key not below the
+//     current k-th key leaves the list unchanged);
+//   - distances use __fmul_rn/__fadd_rn so no FMA contraction can change
+//     a bit, matching the reference's ((dx*dx+dy*dy)+dz*dz) evaluation.
+#include <algorithm>
+
+#include "common.cuh"
+#include "query.cuh"
+
+namespace ckb {
+namespace query {
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+template <int SC, int D, bool EXPL, bool VEC16, int METHOD, class Res>
+__global__ void __launch_bounds__(128) query_kernel(QArgs a)
+{
+  using Tr = Traits<SC>;
+  using T = typename Tr::T;
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= a.nq) return;
+  const int64_t qi = a.order ? int64_t(a.order[i]) : i;
+  T q[D];
+  const T *qp = (const T *)a.queries + qi * D;
+#pragma unroll
+  for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
+  NodeReader<SC, D, EXPL, VEC16> rd(a);
+  Res res(a);
+  if (METHOD == CUKD_STACK_BASED)
+    trav_stack_based<SC, D>(res, q, rd, a.n);
+  else if (METHOD == CUKD_STACK_FREE)
+    trav_stack_free<SC, D>(res, q, rd, a.n, a.eps);
+  else
+    trav_cct<SC, D>(res, q, rd, a.n, (const T *)a.bounds);
+  res.write(a, qi);
+}
+
+template <int SC, int D, bool EXPL, bool VEC16, int METHOD, class Res>
+int launch(const QArgs &a, cudaStream_t st)
+{
+  const int bs = a.block_size > 0 ? a.block_size : 128;
+  const int64_t grid = div_up(a.nq, bs);
+  query_kernel<SC, D, EXPL, VEC16, METHOD, Res><<<unsigned(grid), bs, 0, st>>>(a);
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+template <int SC, int D, bool EXPL, bool VEC16, int METHOD>
+int dispatch_res(const QArgs &a, int kind, cudaStream_t st)
+{
+  switch (kind) {
+    case RES_FCP: return launch<SC, D, EXPL, VEC16, METHOD, FcpRes<SC>>(a, st);
+    case RES_FIX4: return launch<SC, D, EXPL, VEC16, METHOD, FixedRes<SC, 4>>(a, st);
+    case RES_FIX8: return launch<SC, D, EXPL, VEC16, METHOD, FixedRes<SC, 8>>(a, st);
+    case RES_FIX16: return launch<SC, D, EXPL, VEC16, METHOD, FixedRes<SC, 16>>(a, st);
+    case RES_FIX32: return launch<SC, D, EXPL, VEC16, METHOD, FixedRes<SC, 32>>(a, st);
+    case RES_HEAP128: return launch<SC, D, EXPL, VEC16, METHOD, HeapRes<SC, 128>>(a, st);
+    case RES_HEAP1024: return launch<SC, D, EXPL, VEC16, METHOD, HeapRes<SC, 1024>>(a, st);
+  }
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+template <int SC, int D, bool EXPL, bool VEC16>
+int dispatch_method(const QArgs &a, int method, int kind, cudaStream_t st)
+{
+  switch (method) {
+    case CUKD_STACK_BASED: return dispatch_res<SC, D, EXPL, VEC16, CUKD_STACK_BASED>(a, kind, st);
+    case CUKD_STACK_FREE: return dispatch_res<SC, D, EXPL, VEC16, CUKD_STACK_FREE>(a, kind, st);
+    case CUKD_CCT: return dispatch_res<SC, D, EXPL, VEC16, CUKD_CCT>(a, kind, st);
+  }
+  return CUKD_ERR_INVALID_ARGUMENT;
+}
+
+template <int SC, int D>
+int dispatch_layout(const QArgs &a, int method, int kind, cudaStream_t st)
+{
+  const bool expl = a.doff >= 0;
+  const bool vec16 = a.stride == 16 && a.poff == 0 && (!expl || a.doff == 12) && D <= 3;
+  if (expl) {
+    if (vec16) return dispatch_method<SC, D, true, true>(a, method, kind, st);
+    return dispatch_method<SC, D, true, false>(a, method, kind, st);
+  }
+  if (vec16) return dispatch_method<SC, D, false, true>(a, method, kind, st);
+  return dispatch_method<SC, D, false, false>(a, method, kind, st);
+}
+
+int run_query(const QArgs &a, int scalar, int D, int method, int kind, cudaStream_t st)
+{
+#define CKB_CASE(SC_, D_) \
+  if (scalar == SC_ && D == D_) return dispatch_layout<SC_, D_>(a, method, kind, st);
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
+  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+#undef CKB_CASE
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+}  // namespace query
+
+int morton_order_impl(const float *pts, int64_t n, int D, const float *bounds, int32_t *perm,
+                      cudaStream_t st, const cukd_mem_resource *mem);
+
+static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout,
+                        const void *d_world_bounds, const void *d_queries, int64_t nq,
+                        const cukd_query_params *p, bool knn, int32_t *ids, void *d2,
+                        void *maxd2, int64_t *visits, cudaStream_t st,
+                        const cukd_mem_resource *mem)
+{
+  using namespace query;
+  Layout L;
+  if (!make_layout(layout, &L) || !p) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq < 0 || n < 0 || n > (int64_t(1) << 31) - 1) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq == 0) return CUKD_OK;
+  if (!d_queries || (!ids && !visits) || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;
+  if (p->method < CUKD_STACK_BASED || p->method > CUKD_CCT) return CUKD_ERR_INVALID_ARGUMENT;
+  if (p->method == CUKD_CCT && !d_world_bounds) return CUKD_ERR_INVALID_ARGUMENT;
+  int kind = RES_FCP;
+  if (knn) {
+    const int k = p->k;
+    if (k < 1 || k > 1024) return CUKD_ERR_INVALID_ARGUMENT;
+    const bool heap = (p->flags & (CUKD_QUERY_FORCE_HEAP | CUKD_QUERY_HEAP_ORDER)) || k > 32;
+    if (heap)
+      kind = k <= 128 ? RES_HEAP128 : RES_HEAP1024;
+    else
+      kind = k <= 4 ? RES_FIX4 : (k <= 8 ? RES_FIX8 : (k <= 16 ? RES_FIX16 : RES_FIX32));
+  }
+  QArgs a = {};
+  a.tree = (const uint8_t *)d_tree;
+  a.n = n;
+  a.stride = L.stride;
+  a.poff = L.poff;
+  a.doff = L.doff;
+  a.dshift = L.dshift;
+  a.dmask = L.dmask;
+  a.bounds = d_world_bounds;
+  a.queries = d_queries;
+  a.nq = nq;
+  a.k = knn ? p->k : 1;
+  a.cutoff = p->cutoff_radius;
+  a.cutoff_d2 = p->cutoff_d2;
+  a.eps = p->eps;
+  a.heap_order = (p->flags & CUKD_QUERY_HEAP_ORDER) != 0;
+  a.out_ids = ids;
+  a.out_d2 = d2;
+  a.out_max = maxd2;
+  a.visits = visits;
+  a.block_size = p->block_size;
+  TempArena arena(st, mem);
+  if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32) {
+    int32_t *perm = nullptr;
+    CKB_TRY(arena.alloc(&perm, nq));
+    CKB_TRY(morton_order_impl((const float *)d_queries, nq, L.D, nullptr, perm, st, mem));
+    a.order = perm;
+  }
+  return run_query(a, L.scalar, L.D, p->method, kind, st);
+}
+
+}  // namespace ckb
+
+extern "C" {
+
+void cukd_query_params_init(cukd_query_params *p)
+{
+  if (!p) return;
+  p->method = CUKD_STACK_BASED;
+  p->k = 8;
+  p->cutoff_radius = __builtin_huge_valf();
+  p->eps = 0.f;
+  p->cutoff_d2 = INT64_MAX;
+  p->flags = CUKD_QUERY_MORTON;
+  p->block_size = 0;
+}
+
+int cukd_fcp(const void *d_tree, int64_t n, const cukd_layout *layout,
+             const void *d_world_bounds, const void *d_queries, int64_t nq,
+             const cukd_query_params *params, int32_t *d_out_ids, void *d_out_d2,
+             cudaStream_t stream, const cukd_mem_resource *mem)
+{
+  return ckb::common_query(d_tree, n, layout, d_world_bounds, d_queries, nq, params, false,
+                           d_out_ids, d_out_d2, nullptr, nullptr, stream, mem);
+}
+
+int cukd_knn(const void *d_tree, int64_t n, const cukd_layout *layout,
+             const void *d_world_bounds, const void *d_queries, int64_t nq,
+             const cukd_query_params *params, int32_t *d_out_ids, void *d_out_d2,
+             void *d_out_max_d2, cudaStream_t stream, const cukd_mem_resource *mem)
+{
+  if (!d_out_ids && nq > 0) return CUKD_ERR_INVALID_ARGUMENT;
+  return ckb::common_query(d_tree, n, layout, d_world_bounds, d_queries, nq, params, true,
+                           d_out_ids, d_out_d2, d_out_max_d2, nullptr, stream, mem);
+}
+
+int cukd_knn_visits(const void *d_tree, int64_t n, const cukd_layout *layout,
+                    const void *d_world_bounds, const void *d_queries, int64_t nq,
+                    const cukd_query_params *params, int64_t *d_out_visits,
+                    cudaStream_t stream, const cukd_mem_resource *mem)
+{
+  if (!d_out_visits && nq > 0) return CUKD_ERR_INVALID_ARGUMENT;
+  return ckb::common_query(d_tree, n, layout, d_world_bounds, d_queries, nq, params,
+                           params && params->k > 0, nullptr, nullptr, nullptr, d_out_visits,
+                           stream, mem);
+}
+
+}  // extern "C"

@@ -1,0 +1,214 @@
+/*
+ * cukd_b200.h -- C ABI of the B200 (sm_100a) k-d tree library.
+ *
+ * A drop-in for the hot path of ingowald/cudaKDTree.  The reference is a
+ * header-only C++ template library with no ABI; every entry point below is
+ * the plain-C, status-returning counterpart of one of its host templates
+ * (cited per declaration, paths relative to the reference project).  The
+ * C++ shim in include/cukd/ keeps the reference's template API and forwards
+ * here; see INTEGRATION.md for the ctypes / C++ bindings.
+ *
+ * Conventions
+ *   - All pointers named d_* are device pointers (cudaMalloc'd or managed).
+ *   - No entry point throws; each returns a cukd_status.  The C++ shim turns
+ *     non-zero statuses into std::runtime_error, like the reference.
+ *   - All work is enqueued on `stream`; entry points do not synchronise the
+ *     stream unless stated (the reference builder_thrust syncs every level).
+ *   - Temporary memory comes from `mem` (NULL = cudaMallocAsync /
+ *     cudaFreeAsync on `stream`), the counterpart of the reference's
+ *     GpuMemoryResource (cukd/helpers.h:30-70).
+ */
+#ifndef CUKD_B200_H
+#define CUKD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#if defined(_WIN32)
+#define CUKD_API __declspec(dllexport)
+#else
+#define CUKD_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUKD_B200_VERSION 1
+
+typedef enum cukd_status {
+  CUKD_OK = 0,
+  CUKD_ERR_INVALID_ARGUMENT = 1,
+  /* explicit split dims requested but no world-bounds buffer given
+   * (cukd/builder_thrust.h:469-473, builder_bitonic.h:367-372) */
+  CUKD_ERR_MISSING_WORLD_BOUNDS = 2,
+  CUKD_ERR_OUT_OF_MEMORY = 3,
+  CUKD_ERR_CUDA = 4,
+  CUKD_ERR_UNSUPPORTED = 5,
+  /* a bounded device-side wait gave up (batched persistent path) */
+  CUKD_ERR_TIMEOUT = 6,
+  /* a spatial-tree traversal exceeded its 50-entry stack
+   * (cukd/knn.h:620-623 prints "STACK OVERFLOW") */
+  CUKD_ERR_STACK_OVERFLOW = 7
+} cukd_status;
+
+/* ------------------------------------------------------------------------
+ * Data description: the C-ABI form of the reference's data_traits
+ * (cukd/data.h:56-112).  A data item is a record of `stride` bytes holding
+ * `num_dims` contiguous 32-bit coordinates at `point_offset`, and -- for
+ * trees with explicit split dimensions (data_traits::has_explicit_dim) -- a
+ * split dimension stored in bits [dim_shift, dim_shift+dim_bits) of the
+ * 32-bit word at `dim_offset` (dim_offset = -1: round-robin dims).
+ *
+ *   float3                         {CUKD_FLOAT32, 3, 12, 0, -1, 0, 0}
+ *   struct {float3 p; int dim;}    {CUKD_FLOAT32, 3, 16, 0, 12, 0, 32}
+ *   struct {float3 p; int payload;} with the dim in payload bits 30..31
+ *                                  {CUKD_FLOAT32, 3, 16, 0, 12, 30, 2}
+ * ------------------------------------------------------------------------ */
+typedef enum cukd_scalar_type { CUKD_FLOAT32 = 0, CUKD_INT32 = 1 } cukd_scalar_type;
+
+typedef struct cukd_layout {
+  int32_t scalar_type;  /* cukd_scalar_type */
+  int32_t num_dims;     /* 2, 3 or 4 */
+  int32_t stride;       /* bytes per record, multiple of 4 */
+  int32_t point_offset; /* byte offset of coordinate 0, multiple of 4 */
+  int32_t dim_offset;   /* byte offset of the dim word, multiple of 4; -1 = none */
+  int32_t dim_shift;    /* dim = (word >> dim_shift) & ((1 << dim_bits) - 1) */
+  int32_t dim_bits;     /* 1..32 */
+} cukd_layout;
+
+/* world bounds: box_t<point_t> (cukd/box.h:35-82) = lower[num_dims] then
+ * upper[num_dims], of the scalar type. */
+
+/* Memory resource: reference GpuMemoryResource (cukd/helpers.h:30-33). */
+typedef struct cukd_mem_resource {
+  void *ctx;
+  int (*alloc)(void *ctx, void **ptr, size_t bytes, cudaStream_t stream); /* 0 = ok */
+  int (*release)(void *ctx, void *ptr, cudaStream_t stream);
+} cukd_mem_resource;
+
+/* ------------------------------------------------------------------------
+ * Left-balanced k-d tree builders
+ * ------------------------------------------------------------------------ */
+typedef enum cukd_builder {
+  /* reference default: builder_thrust (cukd/builder.h:108-152) */
+  CUKD_BUILDER_DEFAULT = 0,
+  CUKD_BUILDER_THRUST = 1,
+  CUKD_BUILDER_BITONIC = 2,
+  CUKD_BUILDER_INPLACE = 3
+} cukd_builder;
+
+/* Builds a left-balanced k-d tree in place: reorders the n records at
+ * d_points so that record i is node i of the implicit tree (children 2i+1,
+ * 2i+2), and -- for explicit-dim layouts -- writes each node's split dim
+ * (the widest extent of its domain).  Writes the world bounds to
+ * d_world_bounds when non-NULL (mandatory for explicit-dim layouts).
+ * The output is the reference's canonical order (buildTree_host /
+ * buildTree_thrust), ties included, whichever builder is named.
+ * Replaces cukd::buildTree (cukd/builder.h:108-152),
+ * buildTree_thrust (cukd/builder_thrust.h:90-110),
+ * buildTree_bitonic (cukd/builder_bitonic.h:83-94),
+ * buildTree_inPlace (cukd/builder_inplace.h:82-102, 474-480).
+ * n < 1 returns CUKD_OK without touching anything (builder_thrust.h:441). */
+CUKD_API int cukd_build_tree(void *d_points, int64_t n, const cukd_layout *layout,
+                    void *d_world_bounds, int builder, cudaStream_t stream,
+                    const cukd_mem_resource *mem);
+
+/* Computes the world bounds of n records into d_world_bounds.
+ * Replaces cukd::computeBounds (cukd/builder_common.h:151-162). */
+CUKD_API int cukd_compute_bounds(const void *d_points, int64_t n, const cukd_layout *layout,
+                        void *d_world_bounds, cudaStream_t stream);
+
+/* Typed convenience forms of cukd_build_tree for the reference's default
+ * data types (cukd/cukd-math.h:42-59: float2/3/4, int2/3/4). */
+CUKD_API int cukd_build_float2(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,
+                      const cukd_mem_resource *mem);
+CUKD_API int cukd_build_float3(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,
+                      const cukd_mem_resource *mem);
+CUKD_API int cukd_build_float4(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,
+                      const cukd_mem_resource *mem);
+CUKD_API int cukd_build_int2(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,
+                    const cukd_mem_resource *mem);
+CUKD_API int cukd_build_int3(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,
+                    const cukd_mem_resource *mem);
+CUKD_API int cukd_build_int4(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,
+                    const cukd_mem_resource *mem);
+
+/* ------------------------------------------------------------------------
+ * Queries over a left-balanced tree (whole-batch launches)
+ * ------------------------------------------------------------------------ */
+typedef enum cukd_method {
+  CUKD_STACK_BASED = 0, /* cukd::stackBased (traverse-default-stack-based.h) */
+  CUKD_STACK_FREE = 1,  /* cukd::stackFree  (traverse-stack-free.h) */
+  CUKD_CCT = 2          /* cukd::cct        (traverse-cct.h) */
+} cukd_method;
+
+enum {
+  /* sort queries along a 30-bit Morton curve before traversal and scatter
+   * results back to the caller's order (results are unchanged) */
+  CUKD_QUERY_MORTON = 1,
+  /* kNN: return the candidate list in the reference HeapCandidateList's
+   * heap order instead of ascending (d2, id) order */
+  CUKD_QUERY_HEAP_ORDER = 2,
+  /* kNN: use the heap candidate list even for small k */
+  CUKD_QUERY_FORCE_HEAP = 4
+};
+
+typedef struct cukd_query_params {
+  int32_t method;        /* cukd_method */
+  int32_t k;             /* kNN only, 1..1024 */
+  float cutoff_radius;   /* float trees: FcpSearchParams::cutOffRadius (INFINITY = none) */
+  float eps;             /* FcpSearchParams::eps, honoured by CUKD_STACK_FREE */
+  int64_t cutoff_d2;     /* int trees: squared cut-off radius (INT64_MAX = none) */
+  int32_t flags;         /* CUKD_QUERY_* */
+  int32_t block_size;    /* 0 = default; else threads per block (autotuner) */
+} cukd_query_params;
+
+/* Default parameters: stack-based, k = 8, no cut-off, Morton on. */
+CUKD_API void cukd_query_params_init(cukd_query_params *p);
+
+/* Find-closest-point for nq queries (point_t[nq]: num_dims contiguous
+ * scalars each).  d_out_ids[i] = node index of the closest point within the
+ * cut-off, -1 if none (cukd/fcp.h:54-163, FCPResult :179-207).  For float
+ * trees d_out_d2 (optional) receives the squared distance as float, for
+ * int trees as int64.  d_world_bounds is required for CUKD_CCT. */
+CUKD_API int cukd_fcp(const void *d_tree, int64_t n, const cukd_layout *layout,
+             const void *d_world_bounds, const void *d_queries, int64_t nq,
+             const cukd_query_params *params, int32_t *d_out_ids, void *d_out_d2,
+             cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* k nearest neighbours (cukd/knn.h:83-199 with FixedCandidateList /
+ * HeapCandidateList semantics, knn.h:214-287).  d_out_ids / d_out_d2 are
+ * [nq][k]; unfilled slots hold id -1 and d2 = cutoff^2 (knn.h:505-511).
+ * d_out_max_d2 (optional, [nq]) receives knn()'s return value.  float trees
+ * write float d2, int trees int64 d2. */
+CUKD_API int cukd_knn(const void *d_tree, int64_t n, const cukd_layout *layout,
+             const void *d_world_bounds, const void *d_queries, int64_t nq,
+             const cukd_query_params *params, int32_t *d_out_ids, void *d_out_d2,
+             void *d_out_max_d2, cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* Per-query visited-node counts of the same traversal (the reference's
+ * CUKD_ENABLE_STATS counter, cukd/common.h:345-360, per query). */
+CUKD_API int cukd_knn_visits(const void *d_tree, int64_t n, const cukd_layout *layout,
+                    const void *d_world_bounds, const void *d_queries, int64_t nq,
+                    const cukd_query_params *params, int64_t *d_out_visits,
+                    cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* Morton-order permutation of nq float points (30-bit codes inside the
+ * given bounds): d_out_perm[i] = index of the i-th query along the curve. */
+CUKD_API int cukd_morton_order(const float *d_points, int64_t n, int num_dims,
+                      const float *d_bounds, int32_t *d_out_perm, cudaStream_t stream,
+                      const cukd_mem_resource *mem);
+
+/* ------------------------------------------------------------------------
+ * Error strings
+ * ------------------------------------------------------------------------ */
+CUKD_API const char *cukd_status_string(int status);
+/* the CUDA error behind the last CUKD_ERR_CUDA on this thread */
+CUKD_API const char *cukd_last_cuda_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUKD_B200_H */

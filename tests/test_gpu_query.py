@@ -1,0 +1,184 @@
+"""GPU parity of the FCP / kNN traversals against the CPU oracle.
+
+Bar: bit-exact ids AND squared-distance bits for every query, for the three
+traversals (stackBased / stackFree / cct), fixed and heap candidate lists,
+cut-offs, Morton reordering on and off, round-robin and explicit dims,
+float and int coordinates.  The reference's own query test
+(testing/floatN-knn-and-fcp.cu) only compares distances against brute force
+within 1e-6; this is strictly tighter.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import cudakdtree_b200 as ck
+from oracle import pyoracle as po
+from tests.helpers import f32_bits, make_points, make_queries
+
+pytestmark = pytest.mark.gpu
+
+METHODS = [("stack_based", po.STACK_BASED), ("stack_free", po.STACK_FREE), ("cct", po.CCT)]
+
+
+def _tree(n, D, kind, explicit=False, scalar="float32", seed=0):
+    pts = make_points(n, D, kind, scalar=scalar, seed=seed)
+    perm, dims, bounds = po.build(pts, explicit_dim=explicit)
+    return pts[perm], (dims if explicit else None), bounds
+
+
+def _gpu_tree(tree, dims):
+    n, D = tree.shape
+    if dims is None:
+        return torch.from_numpy(np.ascontiguousarray(tree)).cuda(), ck.infer_layout(
+            torch.from_numpy(tree))
+    rec = np.zeros((n, D + 1), np.int32)
+    rec[:, :D] = tree.view(np.int32)
+    rec[:, D] = dims
+    sc = "float32" if tree.dtype == np.float32 else "int32"
+    return torch.from_numpy(rec).cuda(), ck.layout_for(sc, D, stride=4 * (D + 1),
+                                                       dim_offset=4 * D)
+
+
+@pytest.mark.parametrize("mname,m", METHODS)
+@pytest.mark.parametrize("kind", ["uniform", "tie", "gmm"])
+@pytest.mark.parametrize("explicit", [False, True])
+@pytest.mark.parametrize("cutoff", [math.inf, 0.05])
+@pytest.mark.parametrize("morton", [True, False])
+def test_fcp(mname, m, kind, explicit, cutoff, morton):
+    n, nq = 20000, 30000
+    tree, dims, bounds = _tree(n, 3, kind, explicit, seed=1)
+    q = make_queries(nq, 3, kind, seed=2)
+    ref, vis = po.fcp(tree, q, m, dims=dims, bounds=bounds, cutoff=cutoff, visits=True)
+    t, lay = _gpu_tree(tree, dims)
+    wb = torch.from_numpy(bounds).cuda()
+    ids, d2 = ck.fcp(t, torch.from_numpy(q).cuda(), mname, layout=lay, world_bounds=wb,
+                     cutoff=cutoff, morton=morton, with_d2=True)
+    ids = ids.cpu().numpy()
+    assert np.array_equal(ids, ref)
+    d2 = d2.cpu().numpy()
+    has = ref >= 0
+    exp = ((tree[ref[has]] - q[has]) ** 2)
+    # the d2 output is the traversal's own float sum; compare bits with the
+    # oracle's left-to-right float evaluation
+    e = np.zeros(has.sum(), np.float32)
+    for d in range(3):
+        e = (e + exp[:, d].astype(np.float32)).astype(np.float32)
+    assert np.array_equal(f32_bits(d2[has]), f32_bits(e))
+
+
+@pytest.mark.parametrize("mname,m", METHODS)
+@pytest.mark.parametrize("k", [1, 4, 5, 8, 16, 20, 32, 50, 64])
+@pytest.mark.parametrize("kind", ["uniform", "tie"])
+def test_knn(mname, m, k, kind):
+    n, nq = 20000, 8000
+    tree, dims, bounds = _tree(n, 3, kind, False, seed=4)
+    q = make_queries(nq, 3, kind, seed=5)
+    ri, rd, rr = po.knn(tree, q, k, m, bounds=bounds)
+    t, lay = _gpu_tree(tree, dims)
+    wb = torch.from_numpy(bounds).cuda()
+    ids, d2, mx = ck.knn(t, torch.from_numpy(q).cuda(), k, mname, layout=lay, world_bounds=wb,
+                         with_max=True)
+    assert np.array_equal(ids.cpu().numpy(), ri)
+    assert np.array_equal(f32_bits(d2.cpu().numpy()), f32_bits(rd))
+    assert np.array_equal(f32_bits(mx.cpu().numpy()), f32_bits(rr))
+
+
+@pytest.mark.parametrize("mname,m", METHODS)
+@pytest.mark.parametrize("k", [8, 20, 64])
+def test_knn_heap_order(mname, m, k):
+    """HeapCandidateList returns its heap layout (knn.h:427-493)."""
+    n, nq = 5000, 3000
+    tree, dims, bounds = _tree(n, 3, "tie", False, seed=6)
+    q = make_queries(nq, 3, "tie", seed=7)
+    ri, rd, _ = po.knn(tree, q, k, m, bounds=bounds, list_kind=po.HEAP_LIST)
+    t, lay = _gpu_tree(tree, dims)
+    ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), k, mname, layout=lay,
+                     world_bounds=torch.from_numpy(bounds).cuda(), heap_order=True)
+    assert np.array_equal(ids.cpu().numpy(), ri)
+    assert np.array_equal(f32_bits(d2.cpu().numpy()), f32_bits(rd))
+
+
+@pytest.mark.parametrize("mname,m", METHODS)
+@pytest.mark.parametrize("explicit", [False, True])
+@pytest.mark.parametrize("D", [2, 4])
+@pytest.mark.parametrize("cutoff", [math.inf, 0.1])
+def test_knn_dims_cutoff(mname, m, explicit, D, cutoff):
+    n, nq, k = 10000, 5000, 8
+    tree, dims, bounds = _tree(n, D, "uniform", explicit, seed=D)
+    q = make_queries(nq, D, "uniform", seed=D + 1)
+    ri, rd, _ = po.knn(tree, q, k, m, dims=dims, bounds=bounds, cutoff=cutoff)
+    t, lay = _gpu_tree(tree, dims)
+    ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), k, mname, layout=lay,
+                     world_bounds=torch.from_numpy(bounds).cuda(), cutoff=cutoff)
+    assert np.array_equal(ids.cpu().numpy(), ri)
+    assert np.array_equal(f32_bits(d2.cpu().numpy()), f32_bits(rd))
+
+
+@pytest.mark.parametrize("mname,m", METHODS)
+@pytest.mark.parametrize("k", [1, 8, 64])
+@pytest.mark.parametrize("explicit", [False, True])
+def test_int_coordinates(mname, m, k, explicit):
+    """int32 trees: exact int64 squared distances (no reference traversal
+    exists for integer points; the oracle restates the same algorithm)."""
+    n, nq = 20000, 6000
+    tree, dims, bounds = _tree(n, 3, "uniform", explicit, scalar="int32", seed=8)
+    q = make_queries(nq, 3, "uniform", scalar="int32", seed=9)
+    ri, rd, _ = po.knn(tree, q, k, m, dims=dims, bounds=bounds)
+    t, lay = _gpu_tree(tree, dims)
+    ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), k, mname, layout=lay,
+                     world_bounds=torch.from_numpy(bounds).cuda())
+    assert np.array_equal(ids.cpu().numpy(), ri)
+    assert np.array_equal(d2.cpu().numpy(), rd)
+    fi = ck.fcp(t, torch.from_numpy(q).cuda(), mname, layout=lay,
+                world_bounds=torch.from_numpy(bounds).cuda())
+    assert np.array_equal(fi.cpu().numpy(), po.fcp(tree, q, m, dims=dims, bounds=bounds))
+
+
+@pytest.mark.parametrize("eps", [0.0, 0.5])
+def test_stack_free_eps(eps):
+    """FcpSearchParams::eps, honoured by the stack-free traversal only
+    (traverse-stack-free.h:37,85)."""
+    tree, dims, bounds = _tree(20000, 3, "uniform", False, seed=10)
+    q = make_queries(10000, 3, "uniform", seed=11)
+    ref = po.fcp(tree, q, po.STACK_FREE, bounds=bounds, eps=eps)
+    ids = ck.fcp(torch.from_numpy(tree).cuda(), torch.from_numpy(q).cuda(), "stack_free",
+                 eps=eps)
+    assert np.array_equal(ids.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3])
+@pytest.mark.parametrize("mname,m", METHODS)
+def test_tiny_trees(n, mname, m):
+    pts = make_points(max(n, 1), 3, "uniform", seed=12)[:n]
+    if n:
+        perm, _, bounds = po.build(pts)
+        tree = pts[perm]
+    else:
+        tree, bounds = pts, np.zeros((2, 3), np.float32)
+    q = make_queries(100, 3, "uniform", seed=13)
+    ref = po.fcp(tree, q, m, bounds=bounds)
+    t = torch.from_numpy(np.ascontiguousarray(tree)).cuda()
+    ids = ck.fcp(t, torch.from_numpy(q).cuda(), mname, layout=ck.layout_for("float32", 3),
+                 world_bounds=torch.from_numpy(bounds).cuda(), n=n)
+    assert np.array_equal(ids.cpu().numpy(), ref)
+    ri, rd, _ = po.knn(tree, q, 4, m, bounds=bounds)
+    ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), 4, mname, layout=ck.layout_for("float32", 3),
+                     world_bounds=torch.from_numpy(bounds).cuda(), n=n)
+    assert np.array_equal(ids.cpu().numpy(), ri)
+
+
+def test_visits_match_oracle():
+    tree, dims, bounds = _tree(50000, 3, "gmm", False, seed=14)
+    q = make_queries(20000, 3, "gmm", seed=15)
+    _, _, _, vis = po.knn(tree, q, 16, po.STACK_BASED, bounds=bounds, visits=True)
+    v = ck.knn_visits(torch.from_numpy(tree).cuda(), torch.from_numpy(q).cuda(), 16,
+                      "stack_based")
+    assert np.array_equal(v.cpu().numpy(), vis)
+
+
+def test_morton_order_is_a_permutation():
+    q = make_queries(100003, 3, "gmm", seed=16)
+    perm = ck.morton_order(torch.from_numpy(q).cuda()).cpu().numpy()
+    assert np.array_equal(np.sort(perm), np.arange(len(q)))
