@@ -39,7 +39,7 @@ STACK_BASED, STACK_FREE, CCT = 0, 1, 2
 METHODS = {"stack_based": STACK_BASED, "stackBased": STACK_BASED, "stack_free": STACK_FREE,
            "stackFree": STACK_FREE, "cct": CCT}
 BUILDERS = {"default": 0, "thrust": 1, "bitonic": 2, "inplace": 3, "inPlace": 3}
-QUERY_MORTON, QUERY_HEAP_ORDER, QUERY_FORCE_HEAP = 1, 2, 4
+QUERY_MORTON, QUERY_HEAP_ORDER, QUERY_FORCE_HEAP, QUERY_REFERENCE_ORDER = 1, 2, 4, 8
 INT64_MAX = (1 << 63) - 1
 
 
@@ -71,7 +71,7 @@ class Layout(C.Structure):
 class QueryParams(C.Structure):
     _fields_ = [("method", C.c_int32), ("k", C.c_int32), ("cutoff_radius", C.c_float),
                 ("eps", C.c_float), ("cutoff_d2", C.c_int64), ("flags", C.c_int32),
-                ("block_size", C.c_int32)]
+                ("block_size", C.c_int32), ("d_reordered_count", C.c_void_p)]
 
 
 def layout_for(scalar="float32", num_dims=3, stride=None, point_offset=0, dim_offset=-1,
@@ -109,6 +109,7 @@ def lib():
         L.cukd_status_string.argtypes = [C.c_int]
         L.cukd_status_string.restype = C.c_char_p
         L.cukd_last_cuda_error.restype = C.c_char_p
+        L.cukd_launch_count.restype = C.c_ulonglong
         for name in ("cukd_build_float2", "cukd_build_float3", "cukd_build_float4",
                      "cukd_build_int2", "cukd_build_int3", "cukd_build_int4"):
             getattr(L, name).argtypes = [P, I64, P, P, P]
@@ -186,7 +187,7 @@ def build_tree(points, layout=None, world_bounds=None, builder="default", stream
 
 
 def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True,
-            heap_order=False, force_heap=False, block_size=0):
+            heap_order=False, force_heap=False, block_size=0, reference_order=False):
     p = QueryParams()
     p.method = METHODS[method] if isinstance(method, str) else int(method)
     p.k = k
@@ -194,14 +195,15 @@ def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=T
     p.eps = eps
     p.cutoff_d2 = cutoff_d2
     p.flags = ((QUERY_MORTON if morton else 0) | (QUERY_HEAP_ORDER if heap_order else 0)
-               | (QUERY_FORCE_HEAP if force_heap else 0))
+               | (QUERY_FORCE_HEAP if force_heap else 0)
+               | (QUERY_REFERENCE_ORDER if reference_order else 0))
     p.block_size = block_size
     return p
 
 
 def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=None,
         cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True, with_d2=False,
-        stream=None, block_size=0):
+        stream=None, block_size=0, reference_order=False):
     """Find-closest-point for each query ([nq, D] tensor of the tree's scalar
     type).  Returns int32 node indices (-1 = none within the cut-off)."""
     layout = layout or infer_layout(tree)
@@ -213,7 +215,8 @@ def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=N
     if with_d2:
         d2 = torch.empty(nq, dtype=torch.float32 if layout.scalar_type == FLOAT32
                          else torch.int64, device=queries.device)
-    p = _params(method, 1, cutoff, eps, cutoff_d2, morton, block_size=block_size)
+    p = _params(method, 1, cutoff, eps, cutoff_d2, morton, block_size=block_size,
+                reference_order=reference_order)
     _check(lib().cukd_fcp(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
                           _ptr(queries.contiguous()), nq, C.byref(p), _ptr(ids), _ptr(d2),
                           _stream(stream), None), "cukd_fcp")
@@ -222,7 +225,8 @@ def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=N
 
 def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
         cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, heap_order=False,
-        force_heap=False, with_max=False, stream=None, block_size=0):
+        force_heap=False, with_max=False, stream=None, block_size=0, out_ids=None,
+        out_d2=None, reference_order=False, reordered_count=None):
     """k nearest neighbours.  Returns (ids [nq,k] int32, d2 [nq,k]) with the
     reference's candidate-list semantics; ascending unless heap_order."""
     layout = layout or infer_layout(tree)
@@ -230,11 +234,14 @@ def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, 
         n = _num_records(tree, layout)
     nq = queries.shape[0]
     dev = queries.device
-    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
     dt = torch.float32 if layout.scalar_type == FLOAT32 else torch.int64
-    d2 = torch.empty((nq, k), dtype=dt, device=dev)
+    ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32, device=dev)
+    d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, device=dev)
     mx = torch.empty(nq, dtype=dt, device=dev) if with_max else None
-    p = _params(method, k, cutoff, 0.0, cutoff_d2, morton, heap_order, force_heap, block_size)
+    p = _params(method, k, cutoff, 0.0, cutoff_d2, morton, heap_order, force_heap, block_size,
+                reference_order)
+    if reordered_count is not None:  # int32 CUDA tensor of one element
+        p.d_reordered_count = reordered_count.data_ptr()
     _check(lib().cukd_knn(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
                           _ptr(queries.contiguous()), nq, C.byref(p), _ptr(ids), _ptr(d2),
                           _ptr(mx), _stream(stream), None), "cukd_knn")
@@ -254,6 +261,11 @@ def knn_visits(tree, queries, k, method="stack_based", layout=None, world_bounds
                                  _ptr(queries.contiguous()), nq, C.byref(p), _ptr(v),
                                  _stream(stream), None), "cukd_knn_visits")
     return v
+
+
+def launch_count():
+    """Kernels launched by the library so far in this process."""
+    return int(lib().cukd_launch_count())
 
 
 def morton_order(points, bounds=None, stream=None):

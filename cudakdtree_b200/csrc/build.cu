@@ -35,14 +35,37 @@
 // Working data are SoA: one uint32 order-preserving key array per
 // dimension plus the input index, ping-ponged between two buffers.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "common.cuh"
 
 namespace ckb {
 
+unsigned long long launch_count();
 static thread_local cudaError_t g_last_cuda = cudaSuccess;
 void set_cuda_error(cudaError_t e) { g_last_cuda = e; }
+static std::atomic<unsigned long long> g_launches{0};
+void keep_default_pool_memory()
+{
+  static thread_local int doneMask[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const int slot = dev & 7, bit = 1 << ((dev >> 3) & 31);
+  if (doneMask[slot] & bit) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  cudaGetLastError();
+  doneMask[slot] |= bit;
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(); }
 const char *last_cuda_error_string() { return cudaGetErrorString(g_last_cuda); }
 
 namespace build {
@@ -1146,5 +1169,7 @@ const char *cukd_status_string(int status)
 }
 
 const char *cukd_last_cuda_error(void) { return ckb::last_cuda_error_string(); }
+
+unsigned long long cukd_launch_count(void) { return ckb::launch_count(); }
 
 }  // extern "C"

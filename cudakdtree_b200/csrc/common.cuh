@@ -15,9 +15,12 @@ namespace ckb {
 // status plumbing
 // ---------------------------------------------------------------------------
 void set_cuda_error(cudaError_t e);
+// number of kernels this library has launched (reported by the benchmark)
+void count_launch();
 
 #define CKB_CHECK_LAUNCH()                           \
   do {                                               \
+    ::ckb::count_launch();                           \
     cudaError_t _e = cudaGetLastError();             \
     if (_e != cudaSuccess) {                         \
       ::ckb::set_cuda_error(_e);                     \
@@ -44,11 +47,19 @@ void set_cuda_error(cudaError_t e);
 // stream-ordered temporaries through the caller's memory resource
 // (reference: GpuMemoryResource, cukd/helpers.h:30-70)
 // ---------------------------------------------------------------------------
+// Keeps memory freed by cudaFreeAsync in the current device's default pool
+// (by default the pool returns it to the driver at every synchronisation,
+// and the next build would map it again).  Per process and device.
+void keep_default_pool_memory();
+
 struct TempArena {
   cudaStream_t stream;
   const cukd_mem_resource *mem;
   std::vector<void *> ptrs;
-  TempArena(cudaStream_t s, const cukd_mem_resource *m) : stream(s), mem(m) {}
+  TempArena(cudaStream_t s, const cukd_mem_resource *m) : stream(s), mem(m)
+  {
+    if (!mem || !mem->alloc) keep_default_pool_memory();
+  }
   ~TempArena() { release_all(); }
   template <typename T>
   int alloc(T **out, size_t count)

@@ -1,0 +1,287 @@
+// Fast exact kNN / FCP over a left-balanced tree, with reference-order
+// fallback.  (float coordinates, D = 2..4, k <= 32)
+//
+// Why the answer can be computed in any visiting order.  The reference's
+// traversals (traverse-default-stack-based.h, traverse-stack-free.h,
+// traverse-cct.h) keep the k smallest (d2, id) keys among the nodes they
+// visit, and skip a subtree only when its plane/corner distance is not below
+// the current cull distance (the k-th key's d2, which never drops below the
+// final k-th d2 X).  A point with d2 < X is therefore always visited, and a
+// point with d2 == X can only be skipped once k keys with d2 <= X are
+// already in the list.  So whenever exactly k points have d2 <= X (the
+// (k+1)-th smallest d2 is strictly greater than X) the reference returns
+// exactly those k points, whatever its visiting order.  The same holds for
+// FCP (FCPResult, fcp.h:179-207) when the smallest d2 is unique.
+//
+// This kernel keeps the k+1 smallest d2 (ties in any order), culls with
+// "<=" so every point with d2 <= its final (k+1)-th distance is seen, and at
+// the end checks that the (k+1)-th d2 is strictly above the k-th.  Queries
+// that fail the check (distance ties at the boundary, or a point at exactly
+// the cut-off radius) are queued and re-run by the reference-order kernel of
+// the requested method, so every answer is bit-identical to the reference.
+//
+// Throughput features (none changes an answer):
+//   - whichever traversal the caller names, subtrees are culled with the
+//     closest-corner bound of traverse_cct, which is far tighter than the
+//     split-plane bound on clustered data (the named traversal still
+//     answers every queued query, in its own order);
+//   - the candidate list is d2-only floats + ids in registers (right-aligned
+//     k+1 live slots in KC registers), no 64-bit compares;
+//   - optional per-query initial cull radius (learned radius proposal).
+#include <algorithm>
+
+#include "common.cuh"
+#include "fast.cuh"
+
+namespace ckb {
+namespace fast {
+
+using query::QArgs;
+
+// One thread per query (queries in Morton order).  Culling uses the
+// closest-corner distance of each subtree's domain box, the bound of
+// traverse_cct (traverse-cct.h:25-99): the far child's box differs from its
+// parent's only in the split dim, so its closest point to the query is the
+// parent's with that coordinate set to the split value.  Corner distances
+// never exceed the distance of any point inside (every term is a rounded
+// difference of a smaller magnitude), so "<=" culling sees every point with
+// d2 <= the final (k+1)-th distance.
+template <int D, bool EXPL, bool VEC16, int KC>
+__global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
+{
+  const QArgs &a = fa.q;
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= a.nq) return;
+  const int64_t myq = a.order ? int64_t(a.order[i]) : i;
+  const int N = int(a.n);
+  const int k = fa.kk;  // live slots: k+1, right-aligned
+  const uint8_t *tree = a.tree;
+
+  float q[D];
+  {
+    const float *qp = (const float *)a.queries + myq * D;
+#pragma unroll
+    for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
+  }
+  float r2 = __fmul_rn(a.cutoff, a.cutoff);
+  if (fa.radius) {
+    const float rr = __fmul_rn(__ldg(fa.radius + myq), fa.radius_scale);
+    const float rb = __fmul_rn(rr, rr);
+    r2 = rb < r2 ? rb : r2;
+  }
+  const float r2init = r2;
+  float e[KC];
+  int id[KC];
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    e[j] = j < KC - (k + 1) ? -1.f : r2;
+    id[j] = -1;
+  }
+  float cull = r2;
+  bool sawInit = false;
+
+  // closest point of the root's box (the world bounds, or all of space)
+  float closest[D];
+  const float *bnd = (const float *)a.bounds;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    float v = q[d];
+    if (bnd) {
+      const float lo = __ldg(bnd + d), hi = __ldg(bnd + D + d);
+      v = v < lo ? lo : v;
+      v = hi < v ? hi : v;
+    }
+    closest[d] = v;
+  }
+  auto dist2 = [&](const float *c) {
+    float s = __fmul_rn(__fsub_rn(c[0], q[0]), __fsub_rn(c[0], q[0]));
+#pragma unroll
+    for (int d = 1; d < D; d++) s = __fadd_rn(s, __fmul_rn(__fsub_rn(c[d], q[d]), __fsub_rn(c[d], q[d])));
+    return s;
+  };
+
+  int nodeSt[32];
+  float cornerSt[32][D];
+  int sp = 0;
+  int curr = (N > 0 && dist2(closest) <= cull) ? 0 : N;
+  for (;;) {
+    if (curr >= N) {
+      bool found = false;
+      while (sp > 0) {
+        --sp;
+#pragma unroll
+        for (int d = 0; d < D; d++) closest[d] = cornerSt[sp][d];
+        if (dist2(closest) <= cull) {
+          curr = nodeSt[sp];
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+    }
+    float p[D];
+    int dim;
+    if (VEC16) {
+      const uint4 v = __ldg((const uint4 *)(tree + int64_t(curr) * 16));
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int d = 0; d < D; d++) p[d] = __uint_as_float(w[d]);
+      dim = EXPL ? int((w[3] >> a.dshift) & a.dmask) : (level_of(curr) % D);
+    } else {
+      const float *c = (const float *)(tree + int64_t(curr) * a.stride + a.poff);
+#pragma unroll
+      for (int d = 0; d < D; d++) p[d] = __ldg(c + d);
+      dim = EXPL ? int((__ldg((const uint32_t *)(tree + int64_t(curr) * a.stride + a.doff)) >>
+                        a.dshift) & a.dmask)
+                 : (level_of(curr) % D);
+    }
+    const float d2 = dist2(p);
+    sawInit |= (d2 == r2init);
+    if (d2 < e[KC - 1]) {
+      float v = d2;
+      int vi = curr;
+#pragma unroll
+      for (int j = 0; j < KC; j++) {
+        const bool lt = v < e[j];
+        const float lo = lt ? v : e[j];
+        const float hi = lt ? e[j] : v;
+        const int ilo = lt ? vi : id[j];
+        const int ihi = lt ? id[j] : vi;
+        e[j] = lo;
+        id[j] = ilo;
+        v = hi;
+        vi = ihi;
+      }
+      cull = e[KC - 1];
+    }
+    float nodeC = p[0], queryC = q[0];
+#pragma unroll
+    for (int d = 1; d < D; d++)
+      if (d == dim) {
+        nodeC = p[d];
+        queryC = q[d];
+      }
+    const bool leftIsClose = queryC < nodeC;
+    const int lChild = 2 * curr + 1;
+    const int farChild = leftIsClose ? lChild + 1 : lChild;
+    if (farChild < N) {
+      float fc[D];
+#pragma unroll
+      for (int d = 0; d < D; d++) fc[d] = d == dim ? nodeC : closest[d];
+      if (dist2(fc) <= cull) {
+#pragma unroll
+        for (int d = 0; d < D; d++) cornerSt[sp][d] = fc[d];
+        nodeSt[sp] = farChild;
+        sp++;
+      }
+    }
+    curr = leftIsClose ? lChild : lChild + 1;
+  }
+
+  // ---- decide: answer now, or queue for the reference-order traversal
+  const float X = e[KC - 2];  // k-th smallest d2
+  const float Y = e[KC - 1];  // (k+1)-th smallest d2
+  const int idX = id[KC - 2];
+  bool ok;
+  if (fa.fcp) {
+    // unique minimum, or nothing below the cut-off (strict '<' in FCPResult)
+    ok = idX < 0 ? !fa.radius : (Y > X);
+  } else if (idX >= 0) {
+    ok = Y > X;  // strict gap at the k-th boundary
+  } else {
+    ok = !fa.radius && !sawInit;  // fewer than k inside the cut-off
+  }
+  if (!(X == X)) ok = false;  // NaN coordinates
+  if (!ok) {
+    const int slot = atomicAdd(fa.fb_count, 1);
+    fa.fb_list[slot] = int32_t(myq);
+    if (fa.status) fa.status[myq] = 1;
+    return;
+  }
+  if (fa.status) fa.status[myq] = 0;
+  if (fa.fcp) {
+    if (a.out_ids) a.out_ids[myq] = idX >= 0 ? idX : -1;
+    if (a.out_d2) ((float *)a.out_d2)[myq] = idX >= 0 ? X : r2init;
+    return;
+  }
+  // the list is sorted by d2; equal-d2 entries must be ordered by id like
+  // the reference's (d2, id) keys -- rare, sorted only when present
+  unsigned long long key[KC];
+  bool anyEq = false;
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    const bool live = j >= KC - 1 - k && j < KC - 1;
+    key[j] = live ? ((unsigned long long)__float_as_uint(e[j]) << 32) | uint32_t(id[j]) : ~0ull;
+    if (live && j + 1 < KC - 1) anyEq |= (e[j] == e[j + 1]);
+  }
+  if (anyEq) {
+#pragma unroll
+    for (int pass = 0; pass < KC; pass++) {
+#pragma unroll
+      for (int j = (pass & 1); j + 1 < KC; j += 2) {
+        const unsigned long long x = key[j], y = key[j + 1];
+        key[j] = x < y ? x : y;
+        key[j + 1] = x < y ? y : x;
+      }
+    }
+  }
+  const int off = anyEq ? 0 : KC - 1 - k;
+  int32_t *oid = a.out_ids ? a.out_ids + myq * k : nullptr;
+  float *od = a.out_d2 ? (float *)a.out_d2 + myq * k : nullptr;
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    const int o = j - off;
+    if (o >= 0 && o < k) {
+      if (oid) oid[o] = int32_t(uint32_t(key[j]));
+      if (od) od[o] = __uint_as_float(uint32_t(key[j] >> 32));
+    }
+  }
+  if (a.out_max) ((float *)a.out_max)[myq] = X;
+}
+
+template <int D, bool EXPL, bool VEC16, int KC>
+int launch_fast(const FastArgs &fa, cudaStream_t st)
+{
+  const int bs = fa.q.block_size > 0 ? fa.q.block_size : 128;
+  knn_fast_kernel<D, EXPL, VEC16, KC><<<unsigned(div_up(fa.q.nq, bs)), bs, 0, st>>>(fa);
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+template <int D, bool EXPL, bool VEC16>
+int dispatch_kc(const FastArgs &fa, cudaStream_t st)
+{
+  const int slots = fa.kk + 1;
+  if (slots <= 2) return launch_fast<D, EXPL, VEC16, 2>(fa, st);
+  if (slots <= 5) return launch_fast<D, EXPL, VEC16, 5>(fa, st);
+  if (slots <= 9) return launch_fast<D, EXPL, VEC16, 9>(fa, st);
+  if (slots <= 17) return launch_fast<D, EXPL, VEC16, 17>(fa, st);
+  if (slots <= 33) return launch_fast<D, EXPL, VEC16, 33>(fa, st);
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+template <int D>
+int dispatch_layout(const FastArgs &fa, cudaStream_t st)
+{
+  const QArgs &a = fa.q;
+  const bool expl = a.doff >= 0;
+  const bool vec16 = a.stride == 16 && a.poff == 0 && (!expl || a.doff == 12) && D <= 3;
+  if (expl) {
+    if (vec16) return dispatch_kc<D, true, true>(fa, st);
+    return dispatch_kc<D, true, false>(fa, st);
+  }
+  if (vec16) return dispatch_kc<D, false, true>(fa, st);
+  return dispatch_kc<D, false, false>(fa, st);
+}
+
+}  // namespace fast
+
+int run_fast(const fast::FastArgs &fa, int D, cudaStream_t st)
+{
+  if (D == 2) return fast::dispatch_layout<2>(fa, st);
+  if (D == 3) return fast::dispatch_layout<3>(fa, st);
+  if (D == 4) return fast::dispatch_layout<4>(fa, st);
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+}  // namespace ckb

@@ -1,0 +1,26 @@
+// Fast exact kNN / FCP path (fast.cu): arguments and launcher.
+#pragma once
+
+#include "query.cuh"
+
+namespace ckb {
+namespace fast {
+
+struct FastArgs {
+  query::QArgs q;       // tree / queries / outputs (ids, d2 [nq][k], max [nq])
+  int kk;               // k (1 for FCP)
+  bool fcp;             // FCP semantics (strict minimum, -1 beyond the cut-off)
+  int *work;            // global chunk counter (zeroed before the launch)
+  int *fb_count;        // fallback queue length (zeroed before the launch)
+  int32_t *fb_list;     // fallback queue (query indices), capacity nq
+  const float *radius;  // optional per-query initial cull radius (before scaling)
+  int32_t *status;      // optional per-query outcome: 0 answered, 1 queued
+  float radius_scale;   // multiplies `radius`
+};
+
+}  // namespace fast
+
+// Launches the fast kernel for float trees with D = 2..4 and k + 1 <= 33.
+int run_fast(const fast::FastArgs &fa, int D, cudaStream_t st);
+
+}  // namespace ckb

@@ -18,6 +18,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "fast.cuh"
 #include "query.cuh"
 
 namespace ckb {
@@ -31,29 +32,32 @@ __global__ void __launch_bounds__(128) query_kernel(QArgs a)
 {
   using Tr = Traits<SC>;
   using T = typename Tr::T;
-  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= a.nq) return;
-  const int64_t qi = a.order ? int64_t(a.order[i]) : i;
-  T q[D];
-  const T *qp = (const T *)a.queries + qi * D;
+  const int64_t limit = a.count_ptr ? int64_t(*a.count_ptr) : a.nq;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < limit;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t qi = a.order ? int64_t(a.order[i]) : i;
+    T q[D];
+    const T *qp = (const T *)a.queries + qi * D;
 #pragma unroll
-  for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
-  NodeReader<SC, D, EXPL, VEC16> rd(a);
-  Res res(a);
-  if (METHOD == CUKD_STACK_BASED)
-    trav_stack_based<SC, D>(res, q, rd, a.n);
-  else if (METHOD == CUKD_STACK_FREE)
-    trav_stack_free<SC, D>(res, q, rd, a.n, a.eps);
-  else
-    trav_cct<SC, D>(res, q, rd, a.n, (const T *)a.bounds);
-  res.write(a, qi);
+    for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
+    NodeReader<SC, D, EXPL, VEC16> rd(a);
+    Res res(a);
+    if (METHOD == CUKD_STACK_BASED)
+      trav_stack_based<SC, D>(res, q, rd, a.n);
+    else if (METHOD == CUKD_STACK_FREE)
+      trav_stack_free<SC, D>(res, q, rd, a.n, a.eps);
+    else
+      trav_cct<SC, D>(res, q, rd, a.n, (const T *)a.bounds);
+    res.write(a, qi);
+  }
 }
 
 template <int SC, int D, bool EXPL, bool VEC16, int METHOD, class Res>
 int launch(const QArgs &a, cudaStream_t st)
 {
   const int bs = a.block_size > 0 ? a.block_size : 128;
-  const int64_t grid = div_up(a.nq, bs);
+  int64_t grid = div_up(a.nq, bs);
+  if (a.count_ptr) grid = std::min<int64_t>(grid, int64_t(kNumSMs) * 16);
   query_kernel<SC, D, EXPL, VEC16, METHOD, Res><<<unsigned(grid), bs, 0, st>>>(a);
   CKB_CHECK_LAUNCH();
   return CUKD_OK;
@@ -113,6 +117,7 @@ int run_query(const QArgs &a, int scalar, int D, int method, int kind, cudaStrea
 int morton_order_impl(const float *pts, int64_t n, int D, const float *bounds, int32_t *perm,
                       cudaStream_t st, const cukd_mem_resource *mem);
 
+
 static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout,
                         const void *d_world_bounds, const void *d_queries, int64_t nq,
                         const cukd_query_params *p, bool knn, int32_t *ids, void *d2,
@@ -165,6 +170,34 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
     CKB_TRY(morton_order_impl((const float *)d_queries, nq, L.D, nullptr, perm, st, mem));
     a.order = perm;
   }
+  // fast exact path (see fast.cu): any visiting order, boundary-tie check,
+  // reference-order re-run of the queued queries
+  const bool fastOk = L.scalar == CUKD_FLOAT32 && !visits && !a.heap_order &&
+                      !(p->flags & CUKD_QUERY_REFERENCE_ORDER) &&
+                      knn && p->k >= 2 && p->k <= 32 && n < (int64_t(1) << 31) - 1;
+  // (FCP and k = 1 stay on the reference traversals: with a single
+  // candidate the split-plane bound is already cheap and the corner
+  // bookkeeping does not pay for itself)
+  if (fastOk) {
+    fast::FastArgs fa = {};
+    fa.q = a;
+    fa.kk = knn ? p->k : 1;
+    fa.fcp = !knn;
+    int *ctr = nullptr;
+    CKB_TRY(arena.alloc(&ctr, 2));
+    CKB_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(int), st));
+    fa.work = ctr;
+    fa.fb_count = ctr + 1;
+    CKB_TRY(arena.alloc(&fa.fb_list, nq));
+    CKB_TRY(run_fast(fa, L.D, st));
+    if (p->d_reordered_count)
+      CKB_CUDA(cudaMemcpyAsync(p->d_reordered_count, fa.fb_count, sizeof(int),
+                               cudaMemcpyDeviceToDevice, st));
+    QArgs b = a;
+    b.order = fa.fb_list;
+    b.count_ptr = fa.fb_count;
+    return run_query(b, L.scalar, L.D, p->method, kind, st);
+  }
   return run_query(a, L.scalar, L.D, p->method, kind, st);
 }
 
@@ -182,6 +215,7 @@ void cukd_query_params_init(cukd_query_params *p)
   p->cutoff_d2 = INT64_MAX;
   p->flags = CUKD_QUERY_MORTON;
   p->block_size = 0;
+  p->d_reordered_count = nullptr;
 }
 
 int cukd_fcp(const void *d_tree, int64_t n, const cukd_layout *layout,

@@ -29,6 +29,7 @@ struct QArgs {
   const float *radius;  // optional per-query initial cull radius (learned path)
   int32_t *flags_out;   // optional per-query status (learned path)
   int block_size;
+  const int *count_ptr;  // optional device-side number of queries in `order`
 };
 
 enum { RES_FCP = 0, RES_FIX4, RES_FIX8, RES_FIX16, RES_FIX32, RES_HEAP128, RES_HEAP1024 };
@@ -49,6 +50,7 @@ template <> struct Traits<0> {
   __device__ static DT key_d2(Key k) { return __uint_as_float(uint32_t(k >> 32)); }
   __device__ static int32_t key_id(Key k) { return int32_t(uint32_t(k)); }
   __device__ static bool less(Key a, Key b) { return a < b; }
+  __device__ static Key min_key() { return 0ull; }  // <= every (d2 >= +0, id) key
   __device__ static DT init_cull(const QArgs &a) { return __fmul_rn(a.cutoff, a.cutoff); }
 };
 // int coordinates: exact int64 squared distances, key = (d2, id) compared
@@ -69,6 +71,7 @@ template <> struct Traits<1> {
   __device__ static DT key_d2(Key k) { return k.d; }
   __device__ static int32_t key_id(Key k) { return int32_t(k.id); }
   __device__ static bool less(Key a, Key b) { return a.d < b.d || (a.d == b.d && a.id < b.id); }
+  __device__ static Key min_key() { return IKey{-1ll, 0u}; }  // below every d2 >= 0
   __device__ static DT init_cull(const QArgs &a) { return a.cutoff_d2; }
 };
 
@@ -146,9 +149,11 @@ struct FcpRes {
   }
 };
 
-// FixedCandidateList<k> (knn.h:503-548) with register capacity KC >= k:
-// holds the KC smallest keys; the first k of them are exactly the
-// reference list's k entries, and slot k-1 is its maxRadius2.
+// FixedCandidateList<k> (knn.h:503-548) in KC >= k registers.  The k live
+// slots are right-aligned: slots [0, KC-k) hold the smallest possible key,
+// so after every insertion the list's last register is the reference
+// list's slot k-1 (its maxRadius2) and every index stays compile-time
+// (a runtime-indexed register array would be demoted to local memory).
 template <int SC, int KC>
 struct FixedRes {
   using Tr = Traits<SC>;
@@ -161,19 +166,12 @@ struct FixedRes {
   __device__ FixedRes(const QArgs &a) : k(a.k), visits(0)
   {
     const Key init = Tr::encode(Tr::init_cull(a), -1);
+    const Key pad = Tr::min_key();
 #pragma unroll
-    for (int i = 0; i < KC; i++) e[i] = init;
+    for (int i = 0; i < KC; i++) e[i] = i < KC - k ? pad : init;
     cull = Tr::key_d2(init);
   }
   __device__ DT init() const { return cull; }
-  __device__ __forceinline__ Key kth() const
-  {
-    Key r = e[0];
-#pragma unroll
-    for (int i = 1; i < KC; i++)
-      if (i == k - 1) r = e[i];
-    return r;
-  }
   __device__ __forceinline__ DT process(int32_t cand, DT d2)
   {
     visits++;
@@ -187,21 +185,22 @@ struct FixedRes {
         e[i] = lo;
         v = hi;
       }
-      cull = Tr::key_d2(kth());
+      cull = Tr::key_d2(e[KC - 1]);
     }
     return cull;
   }
   __device__ void write(const QArgs &a, int64_t qi) const
   {
+    const int off = KC - k;
     if (a.out_ids) {
 #pragma unroll
       for (int i = 0; i < KC; i++)
-        if (i < k) a.out_ids[qi * k + i] = Tr::key_id(e[i]);
+        if (i >= off) a.out_ids[qi * k + (i - off)] = Tr::key_id(e[i]);
     }
     if (a.out_d2) {
 #pragma unroll
       for (int i = 0; i < KC; i++)
-        if (i < k) ((DT *)a.out_d2)[qi * k + i] = Tr::key_d2(e[i]);
+        if (i >= off) ((DT *)a.out_d2)[qi * k + (i - off)] = Tr::key_d2(e[i]);
     }
     if (a.out_max) ((DT *)a.out_max)[qi] = cull;
     if (a.visits) a.visits[qi] = visits;

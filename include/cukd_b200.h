@@ -152,7 +152,12 @@ enum {
    * heap order instead of ascending (d2, id) order */
   CUKD_QUERY_HEAP_ORDER = 2,
   /* kNN: use the heap candidate list even for small k */
-  CUKD_QUERY_FORCE_HEAP = 4
+  CUKD_QUERY_FORCE_HEAP = 4,
+  /* run every query with the reference's own visiting order (by default
+   * queries whose answer cannot depend on the order -- no distance tie at
+   * the k-th boundary -- take a faster traversal; the answers are the same
+   * bits either way) */
+  CUKD_QUERY_REFERENCE_ORDER = 8
 };
 
 typedef struct cukd_query_params {
@@ -163,6 +168,9 @@ typedef struct cukd_query_params {
   int64_t cutoff_d2;     /* int trees: squared cut-off radius (INT64_MAX = none) */
   int32_t flags;         /* CUKD_QUERY_* */
   int32_t block_size;    /* 0 = default; else threads per block (autotuner) */
+  /* optional device int: receives how many queries were re-run in the
+   * reference's visiting order (distance ties at the k-th boundary) */
+  int32_t *d_reordered_count;
 } cukd_query_params;
 
 /* Default parameters: stack-based, k = 8, no cut-off, Morton on. */
@@ -207,6 +215,10 @@ CUKD_API int cukd_morton_order(const float *d_points, int64_t n, int num_dims,
 CUKD_API const char *cukd_status_string(int status);
 /* the CUDA error behind the last CUKD_ERR_CUDA on this thread */
 CUKD_API const char *cukd_last_cuda_error(void);
+/* running count of kernels launched by this library in this process (an
+ * observability counter, like the reference's CUKD_ENABLE_STATS hook,
+ * cukd/common.h:345-360) */
+CUKD_API unsigned long long cukd_launch_count(void);
 
 #ifdef __cplusplus
 }
