@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -1080,6 +1081,166 @@ int bounds_impl(const void *pts, int64_t n, const Layout &L, void *out, cudaStre
   return CUKD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// allocation-free variant of the builder
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory at the point where they need a
+// tree: code running under another framework that owns the whole device
+// through its own pool and forbids allocations it does not track, real-time
+// loops that cannot afford cudaMalloc's latency or its failure at run time,
+// and deployments that must have a fixed device-memory footprint decided at
+// load time.  For them the builder below takes all of its scratch from one
+// file-scope device array of fixed size instead of a memory resource.  The
+// array exists on every GPU that loads this library, until the process
+// exits.  Every call shares it: calls that can overlap on the GPU (different
+// streams, no ordering between them) race on it and must be serialised by
+// the caller.  Everything the build needs zeroed or filled is reset by the
+// call itself, so a call never sees the previous call's contents.
+constexpr int64_t kNoAllocMaxPoints = 262144;  // records per call
+constexpr int kNoAllocMaxStride = 64;          // bytes per record
+constexpr size_t kNoAllocScratchBytes = size_t(40) << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// bump allocator over the static scratch (same interface as TempArena)
+struct StaticCarver {
+  uint8_t *base;
+  size_t cap, used;
+  template <typename T>
+  int alloc(T **out, size_t count)
+  {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (used + bytes > cap) return CUKD_ERR_TOO_LARGE;
+    *out = (T *)(base + used);
+    used += bytes;
+    return CUKD_OK;
+  }
+};
+
+// Device address of the scratch on the current device, looked up once per
+// device (host code may not use the symbol's name as a device address).
+static int noalloc_scratch_ptr(uint8_t **out)
+{
+  static std::mutex mu;
+  static void *ptrs[64] = {};
+  int dev = 0;
+  CKB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return CUKD_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptrs[dev]) {
+    void *p = nullptr;
+    CKB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return CUKD_ERR_CUDA;
+    ptrs[dev] = p;
+  }
+  *out = (uint8_t *)ptrs[dev];
+  return CUKD_OK;
+}
+
+// The launch sequence of build_impl with every buffer carved from the
+// static scratch (and no memory-pool calls).
+template <int SC, int D>
+int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st)
+{
+  const bool explicitDims = L.doff >= 0;
+  StaticCarver arena;
+  CKB_TRY(noalloc_scratch_ptr(&arena.base));
+  arena.cap = kNoAllocScratchBytes;
+  arena.used = 0;
+  Bufs b = {};
+  int G = 0;
+  while (subtree_size((int64_t(1) << G) - 1, n) > kTile) G++;
+  const int64_t capSeg = int64_t(1) << G;
+  for (int x = 0; x < 2; x++) {
+    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.key[x][d], n));
+    CKB_TRY(arena.alloc(&b.idx[x], n));
+  }
+  if (G > 0) {
+    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.ckey[d], n));
+    CKB_TRY(arena.alloc(&b.cidx, n));
+  }
+  CKB_TRY(arena.alloc(&b.perm, n));
+  CKB_TRY(arena.alloc(&b.ndim, n));
+  uint8_t *orig = nullptr;
+  CKB_TRY(arena.alloc(&orig, size_t(n) * L.stride));
+  for (int x = 0; x < 2; x++) {
+    CKB_TRY(arena.alloc(&b.sdim[x], capSeg));
+    CKB_TRY(arena.alloc(&b.sbmin[x], capSeg * D));
+    CKB_TRY(arena.alloc(&b.sbmax[x], capSeg * D));
+    CKB_TRY(arena.alloc(&b.sbox[x], capSeg * 2 * D));
+  }
+  int64_t histCap = 64;
+  for (int lvl = 0; lvl < G; lvl++) {
+    const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
+    const int nb = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
+    histCap = std::max(histCap, (int64_t(1) << lvl) * nb);
+  }
+  CKB_TRY(arena.alloc(&b.hist, histCap));
+  CKB_TRY(arena.alloc(&b.sel, capSeg * 3));
+  CKB_TRY(arena.alloc(&b.cur, capSeg * 3));
+  CKB_TRY(arena.alloc(&b.wbmin, D));
+  CKB_TRY(arena.alloc(&b.wbmax, D));
+
+  // what must start filled / zeroed is reset here, on the caller's stream
+  CKB_CUDA(cudaMemsetAsync(b.perm, 0xff, sizeof(uint32_t) * n, st));
+  CKB_CUDA(cudaMemsetAsync(b.wbmin, 0xff, sizeof(uint32_t) * D, st));
+  CKB_CUDA(cudaMemsetAsync(b.wbmax, 0, sizeof(uint32_t) * D, st));
+  {
+    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 8));
+    extract_kernel<SC, D><<<blocks, 256, 0, st>>>((const uint8_t *)pts, n, L.stride, L.poff,
+                                                  orig, b);
+    CKB_CHECK_LAUNCH();
+  }
+  root_kernel<SC, D><<<1, 32, 0, st>>>(b, worldBounds, explicitDims);
+  CKB_CHECK_LAUNCH();
+  int cb = 0;
+  for (int lvl = 0; lvl < G; lvl++) {
+    const int nseg = 1 << lvl;
+    const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
+    LevelArgs a;
+    a.n = n;
+    a.level = lvl;
+    a.nb = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
+    a.chunksPerSeg = int(div_up(maxSeg, kChunk));
+    a.nseg = nseg;
+    a.cb = cb;
+    CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
+    CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * 2 * nseg * D, st));
+    CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * 2 * nseg * D, st));
+    const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
+    hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    partition_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
+    CKB_CHECK_LAUNCH();
+    cb ^= 1;
+    std::swap(b.sdim[0], b.sdim[1]);
+    std::swap(b.sbmin[0], b.sbmin[1]);
+    std::swap(b.sbmax[0], b.sbmax[1]);
+    std::swap(b.sbox[0], b.sbox[1]);
+  }
+  {
+    const size_t smem = sizeof(SubSmem<D>);
+    CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
+                                                                       explicitDims);
+    CKB_CHECK_LAUNCH();
+  }
+  {
+    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 16));
+    finalize_kernel<<<blocks, 256, 0, st>>>((uint8_t *)pts, orig, b.perm, b.ndim, n, L.stride,
+                                            explicitDims ? L.doff : -1, L.dshift, L.dmask);
+    CKB_CHECK_LAUNCH();
+  }
+  return CUKD_OK;
+}
+
 }  // namespace build
 
 int build_dispatch(void *pts, int64_t n, const Layout &L, void *wb, cudaStream_t st,
@@ -1099,6 +1260,17 @@ int bounds_dispatch(const void *pts, int64_t n, const Layout &L, void *out, cuda
   using namespace build;
 #define CKB_CASE(SC_, D_) \
   if (L.scalar == SC_ && L.D == D_) return bounds_impl<SC_, D_>(pts, n, L, out, st);
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
+  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+#undef CKB_CASE
+  return CUKD_ERR_UNSUPPORTED;
+}
+
+int build_dispatch_static(void *pts, int64_t n, const Layout &L, void *wb, cudaStream_t st)
+{
+  using namespace build;
+#define CKB_CASE(SC_, D_) \
+  if (L.scalar == SC_ && L.D == D_) return build_impl_static<SC_, D_>(pts, n, L, wb, st);
   CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
   CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
 #undef CKB_CASE
@@ -1135,6 +1307,19 @@ int cukd_compute_bounds(const void *d_points, int64_t n, const cukd_layout *layo
   return ckb::bounds_dispatch(d_points, n, L, d_world_bounds, stream);
 }
 
+int cukd_build_tree_noalloc(void *d_points, int64_t n, const cukd_layout *layout,
+                            void *d_world_bounds, cudaStream_t stream)
+{
+  ckb::Layout L;
+  if (!ckb::make_layout(layout, &L)) return CUKD_ERR_INVALID_ARGUMENT;
+  if (n < 1) return CUKD_OK;
+  if (L.doff >= 0 && !d_world_bounds) return CUKD_ERR_MISSING_WORLD_BOUNDS;
+  if (!d_points) return CUKD_ERR_INVALID_ARGUMENT;
+  if (n > ckb::build::kNoAllocMaxPoints || L.stride > ckb::build::kNoAllocMaxStride)
+    return CUKD_ERR_TOO_LARGE;
+  return ckb::build_dispatch_static(d_points, n, L, d_world_bounds, stream);
+}
+
 #define CKB_TYPED(name, SC, D)                                                            \
   int name(void *d_points, int64_t n, void *d_world_bounds, cudaStream_t stream,          \
            const cukd_mem_resource *mem)                                                  \
@@ -1164,6 +1349,9 @@ const char *cukd_status_string(int status)
     case CUKD_ERR_UNSUPPORTED: return "unsupported data layout or size";
     case CUKD_ERR_TIMEOUT: return "device-side wait timed out";
     case CUKD_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+    case CUKD_ERR_TOO_LARGE:
+      return "input larger than the allocation-free builder's static scratch allows (at most "
+             "262144 records of at most 64 bytes per call)";
   }
   return "unknown status";
 }

@@ -50,7 +50,9 @@ typedef enum cukd_status {
   CUKD_ERR_TIMEOUT = 6,
   /* a spatial-tree traversal exceeded its 50-entry stack
    * (cukd/knn.h:620-623 prints "STACK OVERFLOW") */
-  CUKD_ERR_STACK_OVERFLOW = 7
+  CUKD_ERR_STACK_OVERFLOW = 7,
+  /* input exceeds the fixed scratch of cukd_build_tree_noalloc */
+  CUKD_ERR_TOO_LARGE = 8
 } cukd_status;
 
 /* ------------------------------------------------------------------------
@@ -114,6 +116,26 @@ typedef enum cukd_builder {
 CUKD_API int cukd_build_tree(void *d_points, int64_t n, const cukd_layout *layout,
                     void *d_world_bounds, int builder, cudaStream_t stream,
                     const cukd_mem_resource *mem);
+
+/* Allocation-free build: the same tree as cukd_build_tree (same order, same
+ * explicit dims, same world bounds), for callers that cannot allocate device
+ * memory when they build -- code whose device memory is owned by another
+ * framework's pool, real-time loops that cannot risk cudaMalloc's latency or
+ * failure, deployments with a footprint fixed at load time.  No counterpart
+ * in the reference (its builders always allocate through a
+ * GpuMemoryResource).
+ *
+ * All scratch comes from one fixed 40 MiB device array inside this library
+ * (held on every GPU that loads it, until the process exits); the call
+ * allocates and frees nothing.  Limits: n <= 262144 records, stride <= 64
+ * bytes; larger inputs return CUKD_ERR_TOO_LARGE.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture on that device.  All calls
+ * share the array: calls that may run concurrently on the GPU race and must
+ * be ordered by the caller (one stream, or events).  Each call resets the
+ * parts of the array it needs initialised. */
+CUKD_API int cukd_build_tree_noalloc(void *d_points, int64_t n, const cukd_layout *layout,
+                                     void *d_world_bounds, cudaStream_t stream);
 
 /* Computes the world bounds of n records into d_world_bounds.
  * Replaces cukd::computeBounds (cukd/builder_common.h:151-162). */
