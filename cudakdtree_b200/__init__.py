@@ -68,6 +68,13 @@ class Layout(C.Structure):
                 f"dshift={self.dim_shift}, dbits={self.dim_bits})")
 
 
+class SpatialTreeC(C.Structure):
+    """cukd_spatial_tree."""
+    _fields_ = [("nodes", C.c_void_p), ("prim_ids", C.c_void_p), ("data", C.c_void_p),
+                ("num_prims", C.c_int32), ("num_nodes", C.c_int32), ("num_dims", C.c_int32),
+                ("bounds", C.c_float * 8)]
+
+
 class QueryParams(C.Structure):
     _fields_ = [("method", C.c_int32), ("k", C.c_int32), ("cutoff_radius", C.c_float),
                 ("eps", C.c_float), ("cutoff_d2", C.c_int64), ("flags", C.c_int32),
@@ -81,6 +88,47 @@ def layout_for(scalar="float32", num_dims=3, stride=None, point_offset=0, dim_of
     if stride is None:
         stride = 4 * num_dims
     return Layout(sc, num_dims, stride, point_offset, dim_offset, dim_shift, dim_bits)
+
+
+class MemResource(C.Structure):
+    """cukd_mem_resource (the reference's GpuMemoryResource, helpers.h:30-70)."""
+    _fields_ = [("ctx", C.c_void_p), ("alloc", C.c_void_p), ("release", C.c_void_p)]
+
+
+_ALLOC_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_void_p)
+_RELEASE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+
+
+class TorchMemoryResource:
+    """A cukd_mem_resource that allocates through torch's caching allocator,
+    so library-owned arrays (e.g. spatial-tree nodes) are visible as torch
+    tensors."""
+
+    def __init__(self, device=None):
+        self.device = torch.device("cuda" if device is None else device)
+        self.live = {}
+        self._alloc = _ALLOC_FN(self._do_alloc)
+        self._release = _RELEASE_FN(self._do_release)
+        self.struct = MemResource(None, C.cast(self._alloc, C.c_void_p),
+                                  C.cast(self._release, C.c_void_p))
+
+    def _do_alloc(self, ctx, out, nbytes, stream):
+        try:
+            t = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=self.device)
+        except RuntimeError:
+            return 1
+        self.live[t.data_ptr()] = t
+        out[0] = t.data_ptr()
+        return 0
+
+    def _do_release(self, ctx, ptr, stream):
+        self.live.pop(ptr, None)
+        return 0
+
+    def tensor(self, ptr, dtype, count):
+        """The torch tensor viewing `count` elements of an allocation."""
+        base = self.live[ptr]
+        return base[: count * torch.empty((), dtype=dtype).element_size()].view(dtype)
 
 
 _lib = None
@@ -110,6 +158,13 @@ def lib():
         L.cukd_status_string.restype = C.c_char_p
         L.cukd_last_cuda_error.restype = C.c_char_p
         L.cukd_launch_count.restype = C.c_ulonglong
+        L.cukd_spatial_build.argtypes = [P, I64, C.POINTER(Layout), C.c_int,
+                                         C.POINTER(SpatialTreeC), P, C.POINTER(MemResource)]
+        L.cukd_spatial_free.argtypes = [C.POINTER(SpatialTreeC), P, C.POINTER(MemResource)]
+        L.cukd_spatial_fcp.argtypes = [C.POINTER(SpatialTreeC), C.POINTER(Layout), P, I64,
+                                       C.POINTER(QueryParams), P, P, P, P]
+        L.cukd_spatial_knn.argtypes = [C.POINTER(SpatialTreeC), C.POINTER(Layout), P, I64,
+                                       C.POINTER(QueryParams), P, P, P, P]
         for name in ("cukd_build_float2", "cukd_build_float3", "cukd_build_float4",
                      "cukd_build_int2", "cukd_build_int3", "cukd_build_int4"):
             getattr(L, name).argtypes = [P, I64, P, P, P]
@@ -274,3 +329,68 @@ def morton_order(points, bounds=None, stream=None):
     _check(lib().cukd_morton_order(_ptr(points.contiguous()), n, D, _ptr(bounds), _ptr(perm),
                                    _stream(stream), None), "cukd_morton_order")
     return perm
+
+
+# ---------------------------------------------------------------------------
+# spatial k-d tree (reference: cukd/spatial-kdtree.h)
+# ---------------------------------------------------------------------------
+SPATIAL_NODE_BYTES = 12
+
+
+class SpatialKDTree:
+    """A spatial k-d tree whose node and prim-id arrays live in torch memory.
+    `nodes` is a [num_nodes, 3] int32 view of the 12-byte node records
+    ({float pos; u32 offset; u16 count; i16 dim}); `prim_ids` is int32."""
+
+    def __init__(self, points, layout, leaf_threshold=0, stream=None):
+        self.layout = layout
+        self.points = points
+        self.mr = TorchMemoryResource(points.device)
+        self.c = SpatialTreeC()
+        n = _num_records(points, layout)
+        _check(lib().cukd_spatial_build(_ptr(points), n, C.byref(layout), leaf_threshold,
+                                        C.byref(self.c), _stream(stream),
+                                        C.byref(self.mr.struct)), "cukd_spatial_build")
+
+    @property
+    def num_nodes(self):
+        return self.c.num_nodes
+
+    @property
+    def bounds(self):
+        D = self.c.num_dims
+        return [list(self.c.bounds[:D]), list(self.c.bounds[4:4 + D])]
+
+    def nodes(self):
+        return self.mr.tensor(self.c.nodes, torch.int32, 3 * self.c.num_nodes).view(-1, 3)
+
+    def prim_ids(self):
+        return self.mr.tensor(self.c.prim_ids, torch.int32, self.c.num_prims)
+
+    def free(self, stream=None):
+        if self.c.nodes:
+            _check(lib().cukd_spatial_free(C.byref(self.c), _stream(stream),
+                                           C.byref(self.mr.struct)), "cukd_spatial_free")
+
+    def _query(self, fn, queries, p, k, with_d2, stream):
+        nq = queries.shape[0]
+        shape = (nq,) if k is None else (nq, k)
+        ids = torch.empty(shape, dtype=torch.int32, device=queries.device)
+        d2 = torch.empty(shape, dtype=torch.float32, device=queries.device) if with_d2 else None
+        _check(fn(C.byref(self.c), C.byref(self.layout), _ptr(queries.contiguous()), nq,
+                  C.byref(p), _ptr(ids), _ptr(d2), _stream(stream), None), fn.__name__)
+        return (ids, d2) if with_d2 else ids
+
+    def fcp(self, queries, method="cct", cutoff=math.inf, morton=True, stream=None):
+        p = _params(method, 1, cutoff, 0.0, INT64_MAX, morton)
+        return self._query(lib().cukd_spatial_fcp, queries, p, None, False, stream)
+
+    def knn(self, queries, k, method="cct", cutoff=math.inf, morton=True, heap_order=False,
+            stream=None):
+        p = _params(method, k, cutoff, 0.0, INT64_MAX, morton, heap_order)
+        return self._query(lib().cukd_spatial_knn, queries, p, k, True, stream)
+
+
+def spatial_build(points, layout=None, leaf_threshold=0, stream=None):
+    """Spatial k-d tree over `points` (not reordered)."""
+    return SpatialKDTree(points, layout or infer_layout(points), leaf_threshold, stream)

@@ -232,6 +232,59 @@ CUKD_API int cukd_morton_order(const float *d_points, int64_t n, int num_dims,
                       const cukd_mem_resource *mem);
 
 /* ------------------------------------------------------------------------
+ * Spatial k-d tree (reference: cukd/spatial-kdtree.h)
+ * ------------------------------------------------------------------------ */
+/* Node record, byte-identical to SpatialKDTree<>::Node
+ * (cukd/spatial-kdtree.h:69-98): inner nodes have count 0 and their
+ * children at offset / offset+1; leaves list `count` prim ids from
+ * prim_ids[offset]. */
+typedef struct cukd_spatial_node {
+  float pos;
+  uint32_t offset;
+  uint16_t count;
+  int16_t dim;
+} cukd_spatial_node;
+
+typedef struct cukd_spatial_tree {
+  cukd_spatial_node *nodes; /* device, num_nodes entries (owned) */
+  uint32_t *prim_ids;       /* device, num_prims entries (owned) */
+  const void *data;         /* the caller's records, not reordered (borrowed) */
+  int32_t num_prims;
+  int32_t num_nodes;
+  int32_t num_dims;
+  float bounds[8];          /* lower[0..D) at [0], upper[0..D) at [4] */
+} cukd_spatial_tree;
+
+/* Builds a spatial k-d tree over n float records (leaves of at most
+ * leaf_threshold prims; 0 = the reference's default of 8).  Allocates the
+ * node and prim-id arrays through `mem` (free them with cukd_spatial_free);
+ * the records are only read.  Children are numbered in parent order and
+ * degenerate splits alternate prims by prim id, where the reference uses
+ * atomic order; the tree is otherwise the reference's.
+ * Replaces cukd::buildTree(SpatialKDTree&, ...) (cukd/spatial-kdtree.h:113-126,
+ * 632-645).  Synchronises `stream` once per tree level. */
+CUKD_API int cukd_spatial_build(const void *d_points, int64_t n, const cukd_layout *layout,
+                                int leaf_threshold, cukd_spatial_tree *out_tree,
+                                cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* Replaces cukd::free(SpatialKDTree&, ...) (cukd/spatial-kdtree.h:618-630). */
+CUKD_API int cukd_spatial_free(cukd_spatial_tree *tree, cudaStream_t stream,
+                               const cukd_mem_resource *mem);
+
+/* FCP / kNN over a spatial tree, CUKD_STACK_BASED or CUKD_CCT
+ * (cukd/fcp.h:256-427, cukd/knn.h:566-646, 680-752).  Ids are the caller's
+ * record indices.  A query that overflows the reference's 50-entry stack
+ * returns what the reference returns (FCP -1). */
+CUKD_API int cukd_spatial_fcp(const cukd_spatial_tree *tree, const cukd_layout *layout,
+                              const void *d_queries, int64_t nq,
+                              const cukd_query_params *params, int32_t *d_out_ids,
+                              void *d_out_d2, cudaStream_t stream, const cukd_mem_resource *mem);
+CUKD_API int cukd_spatial_knn(const cukd_spatial_tree *tree, const cukd_layout *layout,
+                              const void *d_queries, int64_t nq,
+                              const cukd_query_params *params, int32_t *d_out_ids,
+                              void *d_out_d2, cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* ------------------------------------------------------------------------
  * Error strings
  * ------------------------------------------------------------------------ */
 CUKD_API const char *cukd_status_string(int status);
