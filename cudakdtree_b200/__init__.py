@@ -165,6 +165,17 @@ def lib():
                                        C.POINTER(QueryParams), P, P, P, P]
         L.cukd_spatial_knn.argtypes = [C.POINTER(SpatialTreeC), C.POINTER(Layout), P, I64,
                                        C.POINTER(QueryParams), P, P, P, P]
+        L.cukd_radius_model_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_uint64]
+        L.cukd_radius_model_destroy.argtypes = [C.c_void_p]
+        L.cukd_radius_model_set_grid.argtypes = [C.c_void_p, P, I64, C.POINTER(Layout), P, P]
+        L.cukd_radius_model_train.argtypes = [C.c_void_p, P, P, I64, C.c_int, C.c_int,
+                                              C.c_float, P, P]
+        L.cukd_radius_model_predict.argtypes = [C.c_void_p, P, I64, P, P]
+        L.cukd_radius_model_features.argtypes = [C.c_void_p, P, I64, P, P]
+        L.cukd_radius_model_gradients.argtypes = [C.c_void_p, P, P, I64, P, P, P, P]
+        L.cukd_knn_learned.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
+                                       C.POINTER(QueryParams), C.c_void_p, C.c_float, P, P, P,
+                                       P, P, P, P]
         for name in ("cukd_build_float2", "cukd_build_float3", "cukd_build_float4",
                      "cukd_build_int2", "cukd_build_int3", "cukd_build_int4"):
             getattr(L, name).argtypes = [P, I64, P, P, P]
@@ -394,3 +405,105 @@ class SpatialKDTree:
 def spatial_build(points, layout=None, leaf_threshold=0, stream=None):
     """Spatial k-d tree over `points` (not reordered)."""
     return SpatialKDTree(points, layout or infer_layout(points), leaf_threshold, stream)
+
+
+# ---------------------------------------------------------------------------
+# learned kNN-radius proposal
+# ---------------------------------------------------------------------------
+class RadiusModel:
+    """MLP radius proposal (cukd_radius_model_*): xyz + log occupancy-grid
+    density -> 64 -> 64 -> 1, BF16 weights, trained on the GPU by the
+    library's own kernels on exact k-th distances."""
+
+    NUM_PARAMS = 4545
+
+    def __init__(self, grid_res=64, seed=0):
+        self.h = C.c_void_p()
+        _check(lib().cukd_radius_model_create(C.byref(self.h), grid_res, seed),
+               "cukd_radius_model_create")
+        self.final_loss = None
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().cukd_radius_model_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    def set_grid(self, tree, layout, world_bounds, n=None, stream=None):
+        n = _num_records(tree, layout) if n is None else n
+        wb = (C.c_float * 6)(*[float(v) for v in world_bounds.detach().cpu().reshape(-1)])
+        _check(lib().cukd_radius_model_set_grid(self.h, _ptr(tree), n, C.byref(layout),
+                                                C.cast(wb, C.c_void_p), _stream(stream)),
+               "cukd_radius_model_set_grid")
+
+    def train(self, queries, kth_d2, epochs=10, batch=4096, lr=2e-3, stream=None):
+        loss = C.c_float()
+        _check(lib().cukd_radius_model_train(self.h, _ptr(queries.contiguous()),
+                                             _ptr(kth_d2.contiguous()), queries.shape[0],
+                                             epochs, batch, lr, C.byref(loss), _stream(stream)),
+               "cukd_radius_model_train")
+        self.final_loss = loss.value
+        return loss.value
+
+    def fit(self, tree, train_queries, k, layout=None, world_bounds=None, epochs=10,
+            batch=4096, lr=2e-3, stream=None):
+        # train_queries should follow the distribution the model will serve
+        """Occupancy grid from the tree, exact k-th distances of the training
+        queries from the plain traversal, then training."""
+        layout = layout or infer_layout(tree)
+        if world_bounds is None:
+            world_bounds = compute_bounds(tree, layout)
+        self.set_grid(tree, layout, world_bounds, stream=stream)
+        _, _, kth = knn(tree, train_queries, k, "cct", layout=layout, world_bounds=world_bounds,
+                        with_max=True, stream=stream)
+        return self.train(train_queries, kth, epochs, batch, lr, stream)
+
+    def predict(self, queries, stream=None):
+        r = torch.empty(queries.shape[0], dtype=torch.float32, device=queries.device)
+        _check(lib().cukd_radius_model_predict(self.h, _ptr(queries.contiguous()),
+                                               queries.shape[0], _ptr(r), _stream(stream)),
+               "cukd_radius_model_predict")
+        return r
+
+    def features(self, queries, stream=None):
+        f = torch.empty((queries.shape[0], 4), dtype=torch.float32, device=queries.device)
+        _check(lib().cukd_radius_model_features(self.h, _ptr(queries.contiguous()),
+                                                queries.shape[0], _ptr(f), _stream(stream)),
+               "cukd_radius_model_features")
+        return f
+
+    def gradients(self, features, targets, stream=None):
+        import numpy as np
+        g = np.zeros(self.NUM_PARAMS, np.float32)
+        p = np.zeros(self.NUM_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(lib().cukd_radius_model_gradients(
+            self.h, _ptr(features.contiguous()), _ptr(targets.contiguous()), features.shape[0],
+            g.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p),
+            loss.ctypes.data_as(C.c_void_p), _stream(stream)), "cukd_radius_model_gradients")
+        return g, p, float(loss[0])
+
+
+def knn_learned(tree, queries, k, model, method="stack_based", layout=None, world_bounds=None,
+                n=None, scale=1.2, morton=True, visits=False, status=False, stream=None,
+                out_ids=None, out_d2=None):
+    """kNN seeded by the learned radius: same results as knn().  Returns
+    (ids, d2, fallback[2] int32 tensor, visits or None[, status])."""
+    layout = layout or infer_layout(tree)
+    n = _num_records(tree, layout) if n is None else n
+    nq = queries.shape[0]
+    dev = queries.device
+    ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32, device=dev)
+    d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=torch.float32, device=dev)
+    fb = torch.zeros(2, dtype=torch.int32, device=dev)
+    v = torch.zeros(nq, dtype=torch.int64, device=dev) if visits else None
+    st = torch.zeros(nq, dtype=torch.int32, device=dev) if status else None
+    p = _params(method, k, math.inf, 0.0, INT64_MAX, morton)
+    _check(lib().cukd_knn_learned(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                                  _ptr(queries.contiguous()), nq, C.byref(p), model.h, scale,
+                                  _ptr(ids), _ptr(d2), _ptr(fb), _ptr(st), _ptr(v),
+                                  _stream(stream), None),
+           "cukd_knn_learned")
+    return (ids, d2, fb, v, st) if status else (ids, d2, fb, v)

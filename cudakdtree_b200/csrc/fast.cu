@@ -51,7 +51,8 @@ __global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
 {
   const QArgs &a = fa.q;
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= a.nq) return;
+  const int64_t limit = a.count_ptr ? int64_t(*a.count_ptr) : a.nq;
+  if (i >= limit) return;
   const int64_t myq = a.order ? int64_t(a.order[i]) : i;
   const int N = int(a.n);
   const int k = fa.kk;  // live slots: k+1, right-aligned
@@ -79,6 +80,7 @@ __global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
   }
   float cull = r2;
   bool sawInit = false;
+  int visits = 0;
 
   // closest point of the root's box (the world bounds, or all of space)
   float closest[D];
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
                  : (level_of(curr) % D);
     }
     const float d2 = dist2(p);
+    ++visits;
     sawInit |= (d2 == r2init);
     if (d2 < e[KC - 1]) {
       float v = d2;
@@ -192,6 +195,7 @@ __global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
     ok = !fa.radius && !sawInit;  // fewer than k inside the cut-off
   }
   if (!(X == X)) ok = false;  // NaN coordinates
+  if (a.visits) a.visits[myq] += visits;  // accumulated over chained passes
   if (!ok) {
     const int slot = atomicAdd(fa.fb_count, 1);
     fa.fb_list[slot] = int32_t(myq);

@@ -1,0 +1,656 @@
+// Learned kNN-radius proposal (no reference counterpart; the reference's
+// queries start from the caller's cut-off radius, cukd/knn.h:503-511).
+//
+// A small MLP predicts each query's k-th-neighbour distance from its
+// normalised coordinates and a coarse density feature, log(1 + points in a
+// cell of a res^3 occupancy grid of the tree's points), interpolated
+// trilinearly between the 8 cell centres around the query:
+//     f (4) -> 64 ReLU -> 64 ReLU -> 1   (the log of the distance,
+//                                         standardised over the training set)
+// Weights are kept in BF16 for every forward/backward pass (FP32 master
+// copy for the optimiser), arithmetic accumulates in FP32.  Training uses
+// exact k-th distances the plain traversal computes, Adam, minibatches.
+//
+// Inference feeds the fast exact kernel (fast.cu) a per-query initial cull
+// radius r_hat * scale.  A query that finds at least k points strictly
+// inside that radius has its exact answer (every point nearer than its k-th
+// neighbour was examined); any other query -- fewer than k inside, or a
+// distance tie at the k-th boundary -- is re-run by the plain unbounded
+// traversal, and a boundary tie there by the reference's own visiting
+// order.  So the learned path returns the same bits as the plain one.
+//
+// Kernels (all hand-written, FP32 accumulate over BF16 weights):
+//   grid_count_kernel   occupancy grid of the tree's points
+//   features_kernel     4 features per query
+//   train_kernel        fused forward + backward of a minibatch slice per
+//                       CTA; per-CTA gradient sums merged with atomics
+//   adam_kernel         Adam update of the FP32 master weights, refresh of
+//                       the BF16 copy, gradient reset
+//   infer_kernel        forward pass per query -> radius
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "fast.cuh"
+#include "query.cuh"
+
+struct cukd_radius_model_s;
+
+namespace ckb {
+namespace learned {
+
+constexpr int H = 64;
+constexpr int OW1 = 0;            // [H][4]  W1[j][i]
+constexpr int OB1 = OW1 + 4 * H;  // [H]
+constexpr int OW2 = OB1 + H;      // [H][H]  W2[j][k]: output j, input k
+constexpr int OB2 = OW2 + H * H;  // [H]
+constexpr int OW3 = OB2 + H;      // [H]
+constexpr int OB3 = OW3 + H;      // [1]
+constexpr int NP = OB3 + 1;       // 4545 parameters
+constexpr int S = 32;             // samples per CTA in training
+constexpr int kTrainThreads = 256;
+
+struct Norm {
+  float lo[3], invext[3];
+  int res;
+  float invLogMax;  // 1 / log(1 + max cell count)
+  float tmean, tstd;
+};
+
+struct ModelDev {
+  float *params;          // FP32 master
+  __nv_bfloat16 *wbf;     // BF16 copy used by every pass
+  float *m, *v, *grad;    // Adam state, gradient accumulator
+  uint32_t *grid;         // res^3 counts
+  float *loss;            // per-step loss sums
+};
+
+// log(1 + cell count), trilinearly interpolated between the centres of the
+// 8 cells around the query (a smooth density estimate at grid scale)
+__device__ inline void features(const Norm &nm, const uint32_t *grid, const float *q, float *f)
+{
+  int c0[3];
+  float w[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const float u = __fmul_rn(__fsub_rn(q[d], nm.lo[d]), nm.invext[d]);
+    f[d] = __fsub_rn(__fmul_rn(u, 2.f), 1.f);
+    // position in cell-centre coordinates
+    float c = __fsub_rn(__fmul_rn(u, float(nm.res)), 0.5f);
+    c = fminf(fmaxf(c, 0.f), float(nm.res - 1));
+    int ci = int(c);
+    ci = ci < nm.res - 1 ? ci : nm.res - 1;
+    c0[d] = ci;
+    w[d] = __fsub_rn(c, float(ci));
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int corner = 0; corner < 8; corner++) {
+    int cell = 0;
+    float wt = 1.f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int bit = (corner >> d) & 1;
+      const int ci = min(c0[d] + bit, nm.res - 1);
+      cell = cell * nm.res + ci;
+      wt = __fmul_rn(wt, bit ? w[d] : __fsub_rn(1.f, w[d]));
+    }
+    acc = __fmaf_rn(wt, log1pf(float(__ldg(grid + cell))), acc);
+  }
+  f[3] = __fmul_rn(acc, nm.invLogMax);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void grid_count_kernel(const uint8_t *__restrict__ pts, int64_t n, int stride,
+                                  int poff, Norm nm, uint32_t *grid)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const float *c = (const float *)(pts + i * stride + poff);
+    int cell = 0;
+    for (int d = 0; d < 3; d++) {
+      const float u = __fmul_rn(__fsub_rn(__ldg(c + d), nm.lo[d]), nm.invext[d]);
+      const float cc = __fmul_rn(u, float(nm.res));
+      const int ci = cc >= 0.f ? (cc < float(nm.res) ? int(cc) : nm.res - 1) : 0;
+      cell = cell * nm.res + ci;
+    }
+    atomicAdd(&grid[cell], 1u);
+  }
+}
+
+__global__ void grid_max_kernel(const uint32_t *grid, int64_t cells, uint32_t *out)
+{
+  uint32_t m = 0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < cells;
+       i += int64_t(gridDim.x) * blockDim.x)
+    m = max(m, grid[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void features_kernel(const float *__restrict__ q, int64_t nq, Norm nm,
+                                const uint32_t *grid, float *feat)
+{
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nq) return;
+  float qq[3] = {q[i * 3], q[i * 3 + 1], q[i * 3 + 2]};
+  float f[4];
+  features(nm, grid, qq, f);
+#pragma unroll
+  for (int d = 0; d < 4; d++) feat[i * 4 + d] = f[d];
+}
+
+// targets: standardised log of the k-th distance (from squared distances)
+__global__ void targets_kernel(const float *kth_d2, int64_t nq, float *t)
+{
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nq) return;
+  t[i] = __fmul_rn(0.5f, logf(fmaxf(kth_d2[i], 1e-30f)));
+}
+
+__global__ void normalize_targets_kernel(float *t, int64_t nq, float mean, float invstd)
+{
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nq) return;
+  t[i] = __fmul_rn(__fsub_rn(t[i], mean), invstd);
+}
+
+// ---------------------------------------------------------------------------
+// fused forward + backward over one slice of S samples per CTA
+// ---------------------------------------------------------------------------
+struct TrainSmem {
+  float w1[H][4], b1[H], w2[H][H], b2[H], w3[H], b3;
+  float f[S][4], h1[S][H], h2[S][H], dh2[S][H], dh1[S][H];
+  float y[S], dy[S];
+};
+
+__global__ void __launch_bounds__(kTrainThreads) train_kernel(
+    const __nv_bfloat16 *__restrict__ wbf, const float *__restrict__ feat,
+    const float *__restrict__ tgt, int64_t begin, int64_t count, float gradScale, float *grad,
+    float *lossOut)
+{
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  TrainSmem &M = *reinterpret_cast<TrainSmem *>(smem_raw);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < NP; i += kTrainThreads) {
+    const float w = __bfloat162float(wbf[i]);
+    if (i < OB1) M.w1[(i - OW1) / 4][(i - OW1) % 4] = w;
+    else if (i < OW2) M.b1[i - OB1] = w;
+    else if (i < OB2) M.w2[(i - OW2) / H][(i - OW2) % H] = w;
+    else if (i < OW3) M.b2[i - OB2] = w;
+    else if (i < OB3) M.w3[i - OW3] = w;
+    else M.b3 = w;
+  }
+  const int64_t s0 = begin + int64_t(blockIdx.x) * S;
+  const int64_t left = begin + count - s0;
+  const int ns = left <= 0 ? 0 : (left < S ? int(left) : S);
+  for (int i = tid; i < S * 4; i += kTrainThreads) {
+    const int s = i / 4;
+    M.f[s][i % 4] = s < ns ? feat[(s0 + s) * 4 + i % 4] : 0.f;
+  }
+  __syncthreads();
+  if (ns == 0) return;
+  // layer 1
+  for (int i = tid; i < S * H; i += kTrainThreads) {
+    const int s = i / H, j = i % H;
+    float z = M.b1[j];
+#pragma unroll
+    for (int c = 0; c < 4; c++) z = __fmaf_rn(M.w1[j][c], M.f[s][c], z);
+    M.h1[s][j] = fmaxf(z, 0.f);
+  }
+  __syncthreads();
+  // layer 2
+  for (int i = tid; i < S * H; i += kTrainThreads) {
+    const int s = i / H, j = i % H;
+    float z = M.b2[j];
+#pragma unroll 16
+    for (int c = 0; c < H; c++) z = __fmaf_rn(M.w2[j][c], M.h1[s][c], z);
+    M.h2[s][j] = fmaxf(z, 0.f);
+  }
+  __syncthreads();
+  // output, loss, dL/dy  (one warp per sample group)
+  {
+    const int lane = tid & 31, wid = tid >> 5;
+    for (int s = wid; s < S; s += kTrainThreads / 32) {
+      float p = __fmul_rn(M.w3[lane], M.h2[s][lane]);
+      p = __fmaf_rn(M.w3[lane + 32], M.h2[s][lane + 32], p);
+      for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+      if (lane == 0) {
+        const float y = p + M.b3;
+        const float e = s < ns ? y - tgt[s0 + s] : 0.f;
+        M.y[s] = y;
+        M.dy[s] = 2.f * e * gradScale;
+        if (s < ns && lossOut) atomicAdd(lossOut, e * e);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < S * H; i += kTrainThreads) {
+    const int s = i / H, j = i % H;
+    M.dh2[s][j] = M.h2[s][j] > 0.f ? M.dy[s] * M.w3[j] : 0.f;
+  }
+  __syncthreads();
+  for (int i = tid; i < S * H; i += kTrainThreads) {
+    const int s = i / H, k = i % H;
+    float g = 0.f;
+#pragma unroll 16
+    for (int j = 0; j < H; j++) g = __fmaf_rn(M.w2[j][k], M.dh2[s][j], g);
+    M.dh1[s][k] = M.h1[s][k] > 0.f ? g : 0.f;
+  }
+  __syncthreads();
+  // gradient sums over the slice, merged into the global accumulator
+  for (int i = tid; i < NP; i += kTrainThreads) {
+    float g = 0.f;
+    if (i < OB1) {
+      const int j = (i - OW1) / 4, c = (i - OW1) % 4;
+      for (int s = 0; s < S; s++) g = __fmaf_rn(M.dh1[s][j], M.f[s][c], g);
+    } else if (i < OW2) {
+      const int j = i - OB1;
+      for (int s = 0; s < S; s++) g += M.dh1[s][j];
+    } else if (i < OB2) {
+      const int j = (i - OW2) / H, k = (i - OW2) % H;
+      for (int s = 0; s < S; s++) g = __fmaf_rn(M.dh2[s][j], M.h1[s][k], g);
+    } else if (i < OW3) {
+      const int j = i - OB2;
+      for (int s = 0; s < S; s++) g += M.dh2[s][j];
+    } else if (i < OB3) {
+      const int j = i - OW3;
+      for (int s = 0; s < S; s++) g = __fmaf_rn(M.dy[s], M.h2[s][j], g);
+    } else {
+      for (int s = 0; s < S; s++) g += M.dy[s];
+    }
+    if (g != 0.f) atomicAdd(&grad[i], g);
+  }
+}
+
+__global__ void adam_kernel(float *params, __nv_bfloat16 *wbf, float *m, float *v, float *grad,
+                            float lr, float b1, float b2, float eps, float c1, float c2)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NP) return;
+  const float g = grad[i];
+  const float mi = b1 * m[i] + (1.f - b1) * g;
+  const float vi = b2 * v[i] + (1.f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float p = params[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  params[i] = p;
+  wbf[i] = __float2bfloat16_rn(p);
+  grad[i] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// inference: one thread per query
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) infer_kernel(const __nv_bfloat16 *__restrict__ wbf,
+                                                    const float *__restrict__ q, int64_t nq,
+                                                    Norm nm, const uint32_t *grid,
+                                                    float *radius)
+{
+  __shared__ float w1[H][4], b1[H], w2[H][H], b2[H], w3[H], b3;
+  for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+    const float w = __bfloat162float(wbf[i]);
+    if (i < OB1) w1[(i - OW1) / 4][(i - OW1) % 4] = w;
+    else if (i < OW2) b1[i - OB1] = w;
+    else if (i < OB2) w2[(i - OW2) / H][(i - OW2) % H] = w;
+    else if (i < OW3) b2[i - OB2] = w;
+    else if (i < OB3) w3[i - OW3] = w;
+    else b3 = w;
+  }
+  __syncthreads();
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nq) return;
+  float qq[3] = {__ldg(q + i * 3), __ldg(q + i * 3 + 1), __ldg(q + i * 3 + 2)};
+  float f[4];
+  features(nm, grid, qq, f);
+  float h1[H];
+#pragma unroll
+  for (int j = 0; j < H; j++) {
+    float z = b1[j];
+#pragma unroll
+    for (int c = 0; c < 4; c++) z = __fmaf_rn(w1[j][c], f[c], z);
+    h1[j] = fmaxf(z, 0.f);
+  }
+  float y = b3;
+  for (int j = 0; j < H; j++) {
+    float z = b2[j];
+#pragma unroll
+    for (int c = 0; c < H; c++) z = __fmaf_rn(w2[j][c], h1[c], z);
+    y = __fmaf_rn(w3[j], fmaxf(z, 0.f), y);
+  }
+  radius[i] = expf(__fmaf_rn(y, nm.tstd, nm.tmean));
+}
+
+// deterministic initialisation (He-uniform), a 64-bit LCG seeded by the caller
+static void init_params(std::vector<float> &p, uint64_t seed)
+{
+  uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto uni = [&]() {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    return float((x >> 11) * (1.0 / 9007199254740992.0)) * 2.f - 1.f;
+  };
+  p.assign(NP, 0.f);
+  for (int i = 0; i < 4 * H; i++) p[OW1 + i] = uni() * std::sqrt(6.f / 4.f);
+  for (int i = 0; i < H * H; i++) p[OW2 + i] = uni() * std::sqrt(6.f / float(H));
+  for (int i = 0; i < H; i++) p[OW3 + i] = uni() * std::sqrt(3.f / float(H));
+}
+
+}  // namespace learned
+
+int run_fast(const fast::FastArgs &fa, int D, cudaStream_t st);
+
+}  // namespace ckb
+
+// opaque model handle
+struct cukd_radius_model_s {
+  int device;
+  int k;
+  ckb::learned::Norm norm;
+  ckb::learned::ModelDev d;
+  int trained;
+  float last_loss;
+};
+
+using namespace ckb;
+using namespace ckb::learned;
+
+static int model_alloc(cukd_radius_model_s *m, int res)
+{
+  CKB_CUDA(cudaMalloc(&m->d.params, sizeof(float) * NP));
+  CKB_CUDA(cudaMalloc(&m->d.wbf, sizeof(__nv_bfloat16) * NP));
+  CKB_CUDA(cudaMalloc(&m->d.m, sizeof(float) * NP));
+  CKB_CUDA(cudaMalloc(&m->d.v, sizeof(float) * NP));
+  CKB_CUDA(cudaMalloc(&m->d.grad, sizeof(float) * NP));
+  CKB_CUDA(cudaMalloc(&m->d.grid, sizeof(uint32_t) * size_t(res) * res * res));
+  CKB_CUDA(cudaMalloc(&m->d.loss, sizeof(float) * 2));
+  return CUKD_OK;
+}
+
+extern "C" {
+
+int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t seed)
+{
+  if (!out || grid_res < 1 || grid_res > 256) return CUKD_ERR_INVALID_ARGUMENT;
+  auto *m = new cukd_radius_model_s();
+  CKB_CUDA(cudaGetDevice(&m->device));
+  m->norm.res = grid_res;
+  m->trained = 0;
+  const int rc = model_alloc(m, grid_res);
+  if (rc != CUKD_OK) {
+    cukd_radius_model_destroy((cukd_radius_model *)m);
+    return rc;
+  }
+  std::vector<float> p;
+  init_params(p, seed);
+  std::vector<__nv_bfloat16> pb(NP);
+  for (int i = 0; i < NP; i++) pb[i] = __float2bfloat16_rn(p[i]);
+  CKB_CUDA(cudaMemcpy(m->d.params, p.data(), sizeof(float) * NP, cudaMemcpyHostToDevice));
+  CKB_CUDA(cudaMemcpy(m->d.wbf, pb.data(), sizeof(__nv_bfloat16) * NP, cudaMemcpyHostToDevice));
+  CKB_CUDA(cudaMemset(m->d.m, 0, sizeof(float) * NP));
+  CKB_CUDA(cudaMemset(m->d.v, 0, sizeof(float) * NP));
+  CKB_CUDA(cudaMemset(m->d.grad, 0, sizeof(float) * NP));
+  *out = (cukd_radius_model *)m;
+  return CUKD_OK;
+}
+
+int cukd_radius_model_destroy(cukd_radius_model *model)
+{
+  auto *m = (cukd_radius_model_s *)model;
+  if (!m) return CUKD_OK;
+  for (void *p : {(void *)m->d.params, (void *)m->d.wbf, (void *)m->d.m, (void *)m->d.v,
+                  (void *)m->d.grad, (void *)m->d.grid, (void *)m->d.loss})
+    if (p) cudaFree(p);
+  delete m;
+  return CUKD_OK;
+}
+
+// Occupancy grid of the tree's points inside d_world_bounds (float3 trees).
+int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_points, int64_t n,
+                               const cukd_layout *layout, const float *h_world_bounds,
+                               cudaStream_t st)
+{
+  auto *m = (cukd_radius_model_s *)model;
+  ckb::Layout L;
+  if (!m || !make_layout(layout, &L) || L.scalar != CUKD_FLOAT32 || L.D != 3 ||
+      !h_world_bounds)
+    return CUKD_ERR_INVALID_ARGUMENT;
+  Norm &nm = m->norm;
+  for (int d = 0; d < 3; d++) {
+    const float lo = h_world_bounds[d], hi = h_world_bounds[3 + d];
+    nm.lo[d] = lo;
+    nm.invext[d] = hi > lo ? 1.f / (hi - lo) : 0.f;
+  }
+  const int64_t cells = int64_t(nm.res) * nm.res * nm.res;
+  CKB_CUDA(cudaMemsetAsync(m->d.grid, 0, sizeof(uint32_t) * cells, st));
+  const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(div_up(n, 256), kNumSMs * 8)));
+  grid_count_kernel<<<blocks, 256, 0, st>>>((const uint8_t *)d_points, n, L.stride, L.poff, nm,
+                                            m->d.grid);
+  CKB_CHECK_LAUNCH();
+  uint32_t *mx = nullptr;
+  CKB_CUDA(cudaMallocAsync(&mx, sizeof(uint32_t), st));
+  CKB_CUDA(cudaMemsetAsync(mx, 0, sizeof(uint32_t), st));
+  grid_max_kernel<<<std::max<int64_t>(1, std::min<int64_t>(div_up(cells, 256), 1024)), 256, 0,
+                    st>>>(m->d.grid, cells, mx);
+  CKB_CHECK_LAUNCH();
+  uint32_t hm = 0;
+  CKB_CUDA(cudaMemcpyAsync(&hm, mx, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CKB_CUDA(cudaFreeAsync(mx, st));
+  CKB_CUDA(cudaStreamSynchronize(st));
+  nm.invLogMax = 1.f / std::log1p(float(std::max<uint32_t>(hm, 1)));
+  return CUKD_OK;
+}
+
+// Trains on (queries, exact k-th squared distances): standardises the log
+// distances, then `epochs` passes of Adam over minibatches of `batch`.
+int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
+                            const float *d_kth_d2, int64_t nq, int epochs, int batch, float lr,
+                            float *h_final_loss, cudaStream_t st)
+{
+  auto *m = (cukd_radius_model_s *)model;
+  if (!m || !d_queries || !d_kth_d2 || nq < 2 || epochs < 1 || batch < S || lr <= 0.f)
+    return CUKD_ERR_INVALID_ARGUMENT;
+  TempArena arena(st, nullptr);
+  float *feat = nullptr, *tgt = nullptr;
+  CKB_TRY(arena.alloc(&feat, nq * 4));
+  CKB_TRY(arena.alloc(&tgt, nq));
+  const unsigned nb = unsigned(div_up(nq, 256));
+  features_kernel<<<nb, 256, 0, st>>>(d_queries, nq, m->norm, m->d.grid, feat);
+  CKB_CHECK_LAUNCH();
+  targets_kernel<<<nb, 256, 0, st>>>(d_kth_d2, nq, tgt);
+  CKB_CHECK_LAUNCH();
+  // standardise targets (host statistics; one read of nq floats)
+  std::vector<float> ht(nq);
+  CKB_CUDA(cudaMemcpyAsync(ht.data(), tgt, sizeof(float) * nq, cudaMemcpyDeviceToHost, st));
+  CKB_CUDA(cudaStreamSynchronize(st));
+  double s1 = 0, s2 = 0;
+  for (float v : ht) {
+    s1 += v;
+    s2 += double(v) * v;
+  }
+  const double mean = s1 / nq, var = std::max(1e-12, s2 / nq - mean * mean);
+  m->norm.tmean = float(mean);
+  m->norm.tstd = float(std::sqrt(var));
+  normalize_targets_kernel<<<nb, 256, 0, st>>>(tgt, nq, m->norm.tmean, 1.f / m->norm.tstd);
+  CKB_CHECK_LAUNCH();
+  const size_t smem = sizeof(TrainSmem);
+  CKB_CUDA(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(smem)));
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  int step = 0;
+  CKB_CUDA(cudaMemsetAsync(m->d.loss, 0, sizeof(float) * 2, st));
+  for (int e = 0; e < epochs; e++) {
+    const bool last = e == epochs - 1;
+    for (int64_t b0 = 0; b0 < nq; b0 += batch) {
+      const int64_t cnt = std::min<int64_t>(batch, nq - b0);
+      train_kernel<<<unsigned(div_up(cnt, S)), kTrainThreads, smem, st>>>(
+          m->d.wbf, feat, tgt, b0, cnt, 1.f / float(cnt), m->d.grad, last ? m->d.loss : nullptr);
+      CKB_CHECK_LAUNCH();
+      step++;
+      const float c1 = 1.f - std::pow(b1, float(step)), c2 = 1.f - std::pow(b2, float(step));
+      adam_kernel<<<div_up(NP, 256), 256, 0, st>>>(m->d.params, m->d.wbf, m->d.m, m->d.v,
+                                                   m->d.grad, lr, b1, b2, eps, c1, c2);
+      CKB_CHECK_LAUNCH();
+    }
+  }
+  float hl = 0.f;
+  CKB_CUDA(cudaMemcpyAsync(&hl, m->d.loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+  CKB_CUDA(cudaStreamSynchronize(st));
+  m->last_loss = hl / float(nq);
+  if (h_final_loss) *h_final_loss = m->last_loss;
+  m->trained = 1;
+  return CUKD_OK;
+}
+
+// Per-query predicted k-th-neighbour distance (before the safety scale).
+int cukd_radius_model_predict(const cukd_radius_model *model, const float *d_queries, int64_t nq,
+                              float *d_out_radius, cudaStream_t st)
+{
+  auto *m = (const cukd_radius_model_s *)model;
+  if (!m || (nq > 0 && (!d_queries || !d_out_radius))) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq == 0) return CUKD_OK;
+  infer_kernel<<<unsigned(div_up(nq, 128)), 128, 0, st>>>(m->d.wbf, d_queries, nq, m->norm,
+                                                          m->d.grid, d_out_radius);
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+// Gradient of the mean squared error over one batch of (features, standardised
+// targets) at the current BF16 weights -- for checking against a CPU oracle.
+int cukd_radius_model_gradients(cukd_radius_model *model, const float *d_features,
+                                const float *d_targets, int64_t n, float *h_grad,
+                                float *h_params_bf16, float *h_loss, cudaStream_t st)
+{
+  auto *m = (cukd_radius_model_s *)model;
+  if (!m || !d_features || !d_targets || n < 1) return CUKD_ERR_INVALID_ARGUMENT;
+  const size_t smem = sizeof(TrainSmem);
+  CKB_CUDA(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(smem)));
+  CKB_CUDA(cudaMemsetAsync(m->d.grad, 0, sizeof(float) * NP, st));
+  CKB_CUDA(cudaMemsetAsync(m->d.loss, 0, sizeof(float) * 2, st));
+  train_kernel<<<unsigned(div_up(n, S)), kTrainThreads, smem, st>>>(
+      m->d.wbf, d_features, d_targets, 0, n, 1.f / float(n), m->d.grad, m->d.loss);
+  CKB_CHECK_LAUNCH();
+  if (h_grad)
+    CKB_CUDA(cudaMemcpyAsync(h_grad, m->d.grad, sizeof(float) * NP, cudaMemcpyDeviceToHost, st));
+  if (h_params_bf16) {
+    std::vector<__nv_bfloat16> pb(NP);
+    CKB_CUDA(cudaMemcpyAsync(pb.data(), m->d.wbf, sizeof(__nv_bfloat16) * NP,
+                             cudaMemcpyDeviceToHost, st));
+    CKB_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < NP; i++) h_params_bf16[i] = __bfloat162float(pb[i]);
+  }
+  float hl = 0.f;
+  CKB_CUDA(cudaMemcpyAsync(&hl, m->d.loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+  CKB_CUDA(cudaStreamSynchronize(st));
+  if (h_loss) *h_loss = hl / float(n);
+  CKB_CUDA(cudaMemsetAsync(m->d.grad, 0, sizeof(float) * NP, st));
+  return CUKD_OK;
+}
+
+// Features of a batch of queries (the model's input), for inspection/tests.
+int cukd_radius_model_features(const cukd_radius_model *model, const float *d_queries,
+                               int64_t nq, float *d_out_features, cudaStream_t st)
+{
+  auto *m = (const cukd_radius_model_s *)model;
+  if (!m || nq < 0) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq == 0) return CUKD_OK;
+  features_kernel<<<unsigned(div_up(nq, 256)), 256, 0, st>>>(d_queries, nq, m->norm, m->d.grid,
+                                                              d_out_features);
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+// kNN with the learned radius: same results as cukd_knn (plain), see the
+// file header.  d_out_fallback (optional, device int[2]): queries re-run by
+// the plain traversal, and by the reference's visiting order.  d_visits
+// (optional, device int64[nq], zeroed by the caller): nodes visited per
+// query over all passes.
+int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
+                     const void *d_world_bounds, const void *d_queries, int64_t nq,
+                     const cukd_query_params *p, const cukd_radius_model *model,
+                     float radius_scale, int32_t *d_out_ids, void *d_out_d2,
+                     int32_t *d_out_fallback, int32_t *d_status, int64_t *d_visits,
+                     cudaStream_t st, const cukd_mem_resource *mem)
+{
+  auto *m = (const cukd_radius_model_s *)model;
+  ckb::Layout L;
+  if (!m || !p || !make_layout(layout, &L) || L.scalar != CUKD_FLOAT32 || L.D != 3)
+    return CUKD_ERR_INVALID_ARGUMENT;
+  if (p->k < 2 || p->k > 32 || (p->flags & CUKD_QUERY_HEAP_ORDER) || radius_scale <= 0.f)
+    return CUKD_ERR_UNSUPPORTED;
+  if (nq == 0) return CUKD_OK;
+  if (!d_queries || !d_out_ids || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;
+  TempArena arena(st, mem);
+  float *radius = nullptr;
+  CKB_TRY(arena.alloc(&radius, nq));
+  CKB_TRY(cukd_radius_model_predict(model, (const float *)d_queries, nq, radius, st));
+  query::QArgs a = {};
+  a.tree = (const uint8_t *)d_tree;
+  a.n = n;
+  a.stride = L.stride;
+  a.poff = L.poff;
+  a.doff = L.doff;
+  a.dshift = L.dshift;
+  a.dmask = L.dmask;
+  a.bounds = d_world_bounds;
+  a.queries = d_queries;
+  a.nq = nq;
+  a.k = p->k;
+  a.cutoff = p->cutoff_radius;
+  a.cutoff_d2 = p->cutoff_d2;
+  a.eps = 0.f;
+  a.out_ids = d_out_ids;
+  a.out_d2 = d_out_d2;
+  a.visits = d_visits;
+  a.block_size = p->block_size;
+  if ((p->flags & CUKD_QUERY_MORTON) && nq > 1) {
+    int32_t *perm = nullptr;
+    CKB_TRY(arena.alloc(&perm, nq));
+    CKB_TRY(cukd_morton_order((const float *)d_queries, nq, 3, nullptr, perm, st, mem));
+    a.order = perm;
+  }
+  int *ctr = nullptr;
+  CKB_TRY(arena.alloc(&ctr, 4));
+  CKB_CUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(int), st));
+  int32_t *fb1 = nullptr, *fb2 = nullptr;
+  CKB_TRY(arena.alloc(&fb1, nq));
+  CKB_TRY(arena.alloc(&fb2, nq));
+  // pass 1: learned initial radius
+  fast::FastArgs fa = {};
+  fa.q = a;
+  fa.kk = p->k;
+  fa.work = ctr;
+  fa.fb_count = ctr + 1;
+  fa.fb_list = fb1;
+  fa.radius = radius;
+  fa.radius_scale = radius_scale;
+  fa.status = d_status;
+  CKB_TRY(run_fast(fa, 3, st));
+  // pass 2: plain unbounded traversal of the queries pass 1 could not answer
+  fast::FastArgs fb = fa;
+  fb.radius = nullptr;
+  fb.status = nullptr;
+  fb.q.order = fb1;
+  fb.q.count_ptr = ctr + 1;
+  fb.fb_count = ctr + 2;
+  fb.fb_list = fb2;
+  CKB_TRY(run_fast(fb, 3, st));
+  // pass 3: boundary ties in the reference's visiting order
+  query::QArgs c = a;
+  c.order = fb2;
+  c.count_ptr = ctr + 2;
+  c.visits = nullptr;
+  const int kind = p->k <= 4 ? query::RES_FIX4
+                             : (p->k <= 8 ? query::RES_FIX8
+                                          : (p->k <= 16 ? query::RES_FIX16 : query::RES_FIX32));
+  CKB_TRY(query::run_query(c, CUKD_FLOAT32, 3, p->method, kind, st));
+  if (d_out_fallback)
+    CKB_CUDA(cudaMemcpyAsync(d_out_fallback, ctr + 1, 2 * sizeof(int), cudaMemcpyDeviceToDevice,
+                             st));
+  return CUKD_OK;
+}
+
+}  // extern "C"

@@ -285,6 +285,67 @@ CUKD_API int cukd_spatial_knn(const cukd_spatial_tree *tree, const cukd_layout *
                               void *d_out_d2, cudaStream_t stream, const cukd_mem_resource *mem);
 
 /* ------------------------------------------------------------------------
+ * Learned kNN-radius proposal (no reference counterpart)
+ *
+ * A small MLP (xyz + log density of a res^3 occupancy grid -> 64 -> 64 -> 1,
+ * BF16 weights, FP32 accumulation) predicts each query's k-th-neighbour
+ * distance.  cukd_knn_learned seeds every query's cull radius with the
+ * prediction times a safety scale; queries that find fewer than k points
+ * inside it (or hit an exact distance tie at the k-th boundary) are re-run
+ * by the plain traversal, so its results equal cukd_knn's bit for bit.
+ * float3 trees only.
+ * ------------------------------------------------------------------------ */
+typedef struct cukd_radius_model_s cukd_radius_model;
+
+/* Creates an untrained model (seeded initialisation) on the current device. */
+CUKD_API int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t seed);
+CUKD_API int cukd_radius_model_destroy(cukd_radius_model *model);
+
+/* Builds the occupancy grid from the tree's points inside the world bounds
+ * (h_world_bounds: host float[6], lower xyz then upper xyz). */
+CUKD_API int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_points,
+                                        int64_t n, const cukd_layout *layout,
+                                        const float *h_world_bounds, cudaStream_t stream);
+
+/* Trains on nq queries and their exact k-th squared distances (for example
+ * the knn() return values of cukd_knn): Adam on minibatches, `epochs`
+ * passes; *h_final_loss receives the last epoch's mean squared error on the
+ * standardised log distance. */
+CUKD_API int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
+                                     const float *d_kth_d2, int64_t nq, int epochs, int batch,
+                                     float lr, float *h_final_loss, cudaStream_t stream);
+
+/* Predicted k-th-neighbour distance per query (not squared, not scaled). */
+CUKD_API int cukd_radius_model_predict(const cukd_radius_model *model, const float *d_queries,
+                                       int64_t nq, float *d_out_radius, cudaStream_t stream);
+
+/* The model's 4 input features per query (device float[nq][4]). */
+CUKD_API int cukd_radius_model_features(const cukd_radius_model *model, const float *d_queries,
+                                        int64_t nq, float *d_out_features, cudaStream_t stream);
+
+/* Mean-squared-error gradient over n (features, standardised target) pairs
+ * at the model's current BF16 weights, without updating them; also returns
+ * those weights as floats and the loss (host buffers of 4545 floats).  For
+ * checking the hand-written backward pass against a CPU oracle. */
+CUKD_API int cukd_radius_model_gradients(cukd_radius_model *model, const float *d_features,
+                                         const float *d_targets, int64_t n, float *h_grad,
+                                         float *h_params_bf16, float *h_loss,
+                                         cudaStream_t stream);
+
+/* kNN (k = 2..32) seeded with the learned radius times radius_scale.
+ * d_out_fallback (optional, device int[2]): queries re-run by the plain
+ * traversal, and by the reference's own visiting order.  d_status
+ * (optional, device int[nq]): 0 if the learned pass answered the query, 1 if
+ * it was re-run.  d_visits (optional, device int64[nq], zeroed by the
+ * caller): visited nodes per query, all passes together. */
+CUKD_API int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
+                              const void *d_world_bounds, const void *d_queries, int64_t nq,
+                              const cukd_query_params *params, const cukd_radius_model *model,
+                              float radius_scale, int32_t *d_out_ids, void *d_out_d2,
+                              int32_t *d_out_fallback, int32_t *d_status, int64_t *d_visits,
+                              cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* ------------------------------------------------------------------------
  * Error strings
  * ------------------------------------------------------------------------ */
 CUKD_API const char *cukd_status_string(int status);

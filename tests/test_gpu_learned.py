@@ -1,0 +1,119 @@
+"""Learned kNN-radius proposal: gradients of the hand-written backward pass
+against the CPU oracle (oracle/mlp_oracle.py), results identical to the plain
+traversal, and what the trained network gains over the plain method."""
+import numpy as np
+import pytest
+import torch
+
+import cudakdtree_b200 as ck
+from cudakdtree_b200 import workloads as wl
+from oracle import mlp_oracle
+from oracle import pyoracle as po
+from tests.helpers import f32_bits
+
+pytestmark = pytest.mark.gpu
+
+LAYOUT = ck.layout_for("float32", 3, stride=16, dim_offset=12, dim_shift=30, dim_bits=2)
+
+
+def _tree(n, seed=3):
+    pts = wl.gmm_points(n, seed=seed)
+    rec = torch.from_numpy(wl.packed_records(pts).view(np.int32).reshape(n, 4).copy()).cuda()
+    wb = ck.build_tree(rec, layout=LAYOUT)
+    return pts, rec, wb
+
+
+def test_gradients_match_cpu_oracle():
+    _, rec, wb = _tree(20000)
+    m = ck.RadiusModel(seed=7)
+    m.set_grid(rec, LAYOUT, wb)
+    q = torch.from_numpy(wl.mixed_queries(3000, seed=11)).cuda()
+    f = m.features(q)
+    t = torch.randn(3000, generator=torch.Generator().manual_seed(0)).cuda()
+    g, p, loss = m.gradients(f, t)
+    ref_loss, ref_g = mlp_oracle.loss_and_grad(p, f.cpu().numpy(), t.cpu().numpy())
+    assert abs(loss - ref_loss) <= 1e-4 * max(1.0, abs(ref_loss))
+    # FP32 accumulation vs float64: relative to the gradient's scale
+    scale = np.abs(ref_g).max()
+    assert np.max(np.abs(g - ref_g)) <= 2e-4 * scale
+
+
+def test_training_reduces_loss_and_forward_matches_oracle():
+    _, rec, wb = _tree(50000)
+    m = ck.RadiusModel(seed=1)
+    qtrain = torch.from_numpy(wl.gmm_points(20000, seed=3, sample_seed=21)).cuda()
+    m.set_grid(rec, LAYOUT, wb)
+    _, _, kth = ck.knn(rec, qtrain, 8, "cct", layout=LAYOUT, world_bounds=wb, with_max=True)
+    f = m.features(qtrain)
+    t_raw = 0.5 * torch.log(kth)
+    t = (t_raw - t_raw.mean()) / t_raw.std(unbiased=False)
+    _, _, loss0 = m.gradients(f, t)
+    loss = m.train(qtrain, kth, epochs=8, batch=2048, lr=3e-3)
+    assert loss < 0.5 * loss0
+    # the model's radius prediction is its forward pass de-standardised
+    _, p, _ = m.gradients(f, t)
+    y, _ = mlp_oracle.forward(p, f.cpu().numpy().astype(np.float64))
+    r = m.predict(qtrain).cpu().numpy()
+    mean, std = float(t_raw.mean()), float(t_raw.std(unbiased=False))
+    assert np.allclose(np.log(r), y * std + mean, rtol=0, atol=2e-3)
+
+
+@pytest.mark.parametrize("k", [8, 16, 32])
+@pytest.mark.parametrize("method", ["stack_based", "stack_free", "cct"])
+def test_learned_results_identical_to_plain(k, method):
+    n = 200000
+    _, rec, wb = _tree(n)
+    m = ck.RadiusModel(seed=2)
+    m.fit(rec, torch.from_numpy(wl.gmm_points(50000, seed=3, sample_seed=31)).cuda(), k,
+          layout=LAYOUT, world_bounds=wb, epochs=6, batch=4096)
+    q = torch.from_numpy(wl.mixed_queries(100000, seed=41)).cuda()
+    pi, pd = ck.knn(rec, q, k, method, layout=LAYOUT, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(rec, q, k, m, method, layout=LAYOUT, world_bounds=wb)
+    assert torch.equal(li, pi)
+    assert np.array_equal(f32_bits(ld.cpu().numpy()), f32_bits(pd.cpu().numpy()))
+    # and with the reference traversal order everywhere
+    ri, rd = ck.knn(rec, q, k, method, layout=LAYOUT, world_bounds=wb, reference_order=True)
+    assert torch.equal(li, ri)
+
+
+def test_learned_radius_with_tiny_scale_falls_back_and_stays_exact():
+    """A radius far too small sends (almost) every query to the plain path;
+    the results must not change."""
+    _, rec, wb = _tree(50000)
+    m = ck.RadiusModel(seed=3)
+    m.fit(rec, torch.from_numpy(wl.gmm_points(20000, seed=3, sample_seed=5)).cuda(), 16,
+          layout=LAYOUT, world_bounds=wb, epochs=2)
+    q = torch.from_numpy(wl.mixed_queries(20000, seed=6)).cuda()
+    pi, pd = ck.knn(rec, q, 16, layout=LAYOUT, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(rec, q, 16, m, layout=LAYOUT, world_bounds=wb, scale=1e-3)
+    assert int(fb[0]) > 19000
+    assert torch.equal(li, pi) and torch.equal(ld, pd)
+
+
+def test_trained_network_reduces_work():
+    """What the trained network gains: every query the learned pass answers
+    visits no more nodes than the plain search does (the radius only adds
+    culling), fewer on average, with identical answers; the share of
+    queries re-run stays small."""
+    n = 1000000
+    _, rec, wb = _tree(n)
+    m = ck.RadiusModel(grid_res=64, seed=4)
+    m.fit(rec, torch.from_numpy(wl.mixed_queries(200000, seed=51)).cuda(), 16,
+          layout=LAYOUT, world_bounds=wb, epochs=20, batch=4096)
+    q = torch.from_numpy(wl.mixed_queries(200000, seed=52)).cuda()
+    # the plain fast path with visit counting: an infinite radius scale
+    pi, pd, _, v_plain = ck.knn_learned(rec, q, 16, m, layout=LAYOUT, world_bounds=wb,
+                                        scale=1e30, visits=True)
+    li, ld, fb, v_learn, st = ck.knn_learned(rec, q, 16, m, layout=LAYOUT, world_bounds=wb,
+                                             scale=1.2, visits=True, status=True)
+    assert torch.equal(li, pi) and torch.equal(ld, pd)
+    answered = st == 0
+    frac_fallback = 1.0 - answered.double().mean().item()
+    assert abs(frac_fallback - int(fb[0]) / q.shape[0]) < 1e-9
+    assert torch.all(v_learn[answered] <= v_plain[answered])
+    vp = v_plain[answered].double().mean().item()
+    vl = v_learn[answered].double().mean().item()
+    print(f"fallback {frac_fallback:.3f}  visits of answered queries: plain {vp:.1f} "
+          f"learned {vl:.1f}  final loss {m.final_loss:.4f}")
+    assert frac_fallback < 0.25
+    assert vl < vp

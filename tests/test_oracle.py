@@ -209,3 +209,20 @@ def test_explicit_dims_need_bounds():
     rc = po.lib().cko_build(0, 3, pts.ctypes.data_as(C.c_void_p), 4, 1,
                             perm.ctypes.data_as(C.c_void_p), None, None)
     assert rc == 2
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The MLP oracle's backward pass (the reference point for the GPU
+    training kernels) against central finite differences."""
+    from oracle import mlp_oracle as mo
+    rng = np.random.default_rng(0)
+    p = rng.normal(0, 0.3, mo.NP)
+    f = rng.normal(0, 1, (16, 4))
+    t = rng.normal(0, 1, 16)
+    _, g = mo.loss_and_grad(p, f, t)
+    for i in [0, 5, mo.OB1 + 3, mo.OW2 + 100, mo.OW2 + 4000, mo.OB2 + 7, mo.OW3 + 9, mo.OB3]:
+        e = np.zeros(mo.NP)
+        e[i] = 1e-6
+        lp, _ = mo.loss_and_grad(p + e, f, t)
+        lm, _ = mo.loss_and_grad(p - e, f, t)
+        assert abs((lp - lm) / 2e-6 - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
