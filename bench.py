@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
 
 
@@ -230,8 +231,41 @@ def run_ours(args, rank, world, local):
                                      out_ids=d_ids, out_d2=d_d2))
     knn_sf_ms = timed(lambda: ck.knn(d_pts, d_q, K, "stack_free", layout=lay, world_bounds=wb,
                                      out_ids=d_ids, out_d2=d_d2))
+    knn_ref_ms = timed(lambda: ck.knn(d_pts, d_q, K, "stack_based", layout=lay,
+                                      world_bounds=wb, out_ids=d_ids, out_d2=d_d2,
+                                      reference_order=True), reps=1)
     morton_ms = timed(lambda: ck.morton_order(d_q))
     fcp_ms = timed(lambda: ck.fcp(d_pts, d_q, "stack_based", layout=lay, world_bounds=wb))
+
+    # ---- learned radius vs plain on the same queries (config 4's method on
+    # this workload: trained on 1M queries from the query distribution)
+    learned = None
+    if not args.no_learned:
+        from cudakdtree_b200 import workloads as wl
+        ntrain = min(1_000_000, nq)
+        qtrain = torch.from_numpy(wl.gmm_points(ntrain, seed=3, sample_seed=14)).to(dev)
+        model = ck.RadiusModel(grid_res=64, seed=1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        model.fit(d_pts, qtrain, K, layout=lay, world_bounds=wb, epochs=10, batch=4096)
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        fb = [None]
+
+        def run_learned():
+            fb[0] = ck.knn_learned(d_pts, d_q, K, model, "stack_based", layout=lay,
+                                   world_bounds=wb, scale=1.2, out_ids=d_ids, out_d2=d_d2)[2]
+
+        learned_ms = timed(run_learned)
+        learned = {"knn_ms": round(learned_ms, 3), "plain_knn_ms": round(knn_sb_ms, 3),
+                   "speedup_vs_plain": round(knn_sb_ms / learned_ms, 3),
+                   "reference_order_knn_ms": round(knn_ref_ms, 3),
+                   "speedup_vs_reference_order": round(knn_ref_ms / learned_ms, 3),
+                   "queries_per_s": round(nq / (learned_ms / 1e3), 1),
+                   "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
+                   "reference_order_reruns": int(fb[0][1].item()),
+                   "train_s": round(train_s, 3), "train_queries": ntrain,
+                   "final_loss": round(model.final_loss, 5), "radius_scale": 1.2}
 
     # ---- roofline of the dominant kernel (kNN traversal)
     peak, peak_src = measured_peaks()
@@ -303,9 +337,11 @@ def run_ours(args, rank, world, local):
                       "parallelism": f"replicas x{world}"},
            "phases_ms": {"build": round(build_ms, 3), "knn_stack_based": round(knn_sb_ms, 3),
                          "knn_stack_free": round(knn_sf_ms, 3), "morton_order": round(morton_ms, 3),
-                         "fcp_stack_based": round(fcp_ms, 3), "restore_copy": round(copy_ms, 3)},
+                         "fcp_stack_based": round(fcp_ms, 3), "restore_copy": round(copy_ms, 3),
+                         "knn_stack_based_reference_order": round(knn_ref_ms, 3)},
            "build_ms": round(build_ms, 3),
            "knn_stack_free_queries_per_s": round(nq / (knn_sf_ms / 1e3), 1),
+           "learned_radius": learned,
            "roofline": roofline, "build_roofline": build_roof,
            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
            "gpu_launches_per_step": round(launches / args.steps, 1)}
