@@ -29,6 +29,7 @@ import torch
 __all__ = [
     "lib", "Layout", "layout_for", "build_tree", "compute_bounds", "fcp", "knn",
     "knn_visits", "morton_order", "CukdError", "STACK_BASED", "STACK_FREE", "CCT",
+    "BatchPlan",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -79,6 +80,16 @@ class QueryParams(C.Structure):
     _fields_ = [("method", C.c_int32), ("k", C.c_int32), ("cutoff_radius", C.c_float),
                 ("eps", C.c_float), ("cutoff_d2", C.c_int64), ("flags", C.c_int32),
                 ("block_size", C.c_int32), ("d_reordered_count", C.c_void_p)]
+
+
+class BatchTuning(C.Structure):
+    """cukd_batch_tuning."""
+    _fields_ = [("build_tile", C.c_int32), ("block_size", C.c_int32),
+                ("queries_per_thread", C.c_int32), ("morton", C.c_int32),
+                ("build_ms", C.c_float), ("query_ms", C.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 def layout_for(scalar="float32", num_dims=3, stride=None, point_offset=0, dim_offset=-1,
@@ -176,6 +187,15 @@ def lib():
         L.cukd_knn_learned.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
                                        C.POINTER(QueryParams), C.c_void_p, C.c_float, P, P, P,
                                        P, P, P, P]
+        L.cukd_batch_plan_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, I64, P, P,
+                                             C.POINTER(QueryParams)]
+        L.cukd_batch_plan_destroy.argtypes = [C.c_void_p]
+        L.cukd_batch_get_tuning.argtypes = [C.c_void_p, C.POINTER(BatchTuning)]
+        L.cukd_batch_set_tuning.argtypes = [C.c_void_p, C.POINTER(BatchTuning)]
+        L.cukd_batch_build.argtypes = [C.c_void_p, P, P, P]
+        L.cukd_batch_query.argtypes = [C.c_void_p, P, P, P, P, P, P]
+        L.cukd_batch_run.argtypes = [C.c_void_p, P, P, P, P, P, P]
+        L.cukd_batch_autotune.argtypes = [C.c_void_p, P, P, C.c_int, C.POINTER(BatchTuning), P]
         for name in ("cukd_build_float2", "cukd_build_float3", "cukd_build_float4",
                      "cukd_build_int2", "cukd_build_int3", "cukd_build_int4"):
             getattr(L, name).argtypes = [P, I64, P, P, P]
@@ -507,3 +527,95 @@ def knn_learned(tree, queries, k, model, method="stack_based", layout=None, worl
                                   _stream(stream), None),
            "cukd_knn_learned")
     return (ids, d2, fb, v, st) if status else (ids, d2, fb, v)
+
+
+# ---------------------------------------------------------------------------
+# batched clouds (no reference counterpart)
+# ---------------------------------------------------------------------------
+class BatchPlan:
+    """Many independent float clouds (CSR offsets over one [total, D] array)
+    built into their own left-balanced trees in place and queried with
+    their own query sets (cukd_batch_*).  Results equal a per-cloud loop of
+    build_tree + knn / fcp, ids local to each cloud.  k = 0 means FCP."""
+
+    def __init__(self, point_offsets, query_offsets, num_dims=3, k=8, method="stack_based",
+                 cutoff=math.inf, eps=0.0, heap_order=False, force_heap=False,
+                 reference_order=False):
+        import numpy as np
+        po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.int64))
+        qo = np.ascontiguousarray(np.asarray(query_offsets, dtype=np.int64))
+        if po.ndim != 1 or qo.shape != po.shape or po.size < 1:
+            raise ValueError("point_offsets and query_offsets: int64[B + 1]")
+        self.num_clouds = po.size - 1
+        self.point_offsets, self.query_offsets = po, qo
+        self.num_dims, self.k = num_dims, k
+        self.total, self.nq = int(po[-1]), int(qo[-1])
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        p = _params(m, k, cutoff, eps, INT64_MAX, True, heap_order=heap_order,
+                    force_heap=force_heap, reference_order=reference_order)
+        self.h = C.c_void_p()
+        _check(lib().cukd_batch_plan_create(C.byref(self.h), num_dims, self.num_clouds,
+                                            po.ctypes.data_as(C.c_void_p),
+                                            qo.ctypes.data_as(C.c_void_p), C.byref(p)),
+               "cukd_batch_plan_create")
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().cukd_batch_plan_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    def close(self):
+        self.__del__()
+
+    @property
+    def tuning(self):
+        t = BatchTuning()
+        _check(lib().cukd_batch_get_tuning(self.h, C.byref(t)), "cukd_batch_get_tuning")
+        return t
+
+    def set_tuning(self, build_tile=None, block_size=None, queries_per_thread=None, morton=None):
+        t = self.tuning
+        for name, v in (("build_tile", build_tile), ("block_size", block_size),
+                        ("queries_per_thread", queries_per_thread), ("morton", morton)):
+            if v is not None:
+                setattr(t, name, int(v))
+        _check(lib().cukd_batch_set_tuning(self.h, C.byref(t)), "cukd_batch_set_tuning")
+
+    def _outputs(self, dev):
+        kk = max(self.k, 1)
+        shape = (self.nq, kk) if self.k > 0 else (self.nq,)
+        return (torch.empty(shape, dtype=torch.int32, device=dev),
+                torch.empty(shape, dtype=torch.float32, device=dev))
+
+    def bounds_tensor(self, dev):
+        return torch.empty((self.num_clouds, 2, self.num_dims), dtype=torch.float32, device=dev)
+
+    def build(self, points, bounds=None, stream=None):
+        """Builds every cloud of `points` (float32 [total, D], in place)."""
+        _check(lib().cukd_batch_build(self.h, _ptr(points), _ptr(bounds), _stream(stream)),
+               "cukd_batch_build")
+        return points
+
+    def query(self, points, queries, bounds=None, out=None, stream=None):
+        ids, d2 = out if out is not None else self._outputs(queries.device)
+        _check(lib().cukd_batch_query(self.h, _ptr(points), _ptr(bounds),
+                                      _ptr(queries.contiguous()), _ptr(ids), _ptr(d2),
+                                      _stream(stream)), "cukd_batch_query")
+        return ids, d2
+
+    def run(self, points, queries, bounds=None, out=None, stream=None):
+        """Build + query as one replayed CUDA graph."""
+        ids, d2 = out if out is not None else self._outputs(queries.device)
+        _check(lib().cukd_batch_run(self.h, _ptr(points), _ptr(bounds),
+                                    _ptr(queries.contiguous()), _ptr(ids), _ptr(d2),
+                                    _stream(stream)), "cukd_batch_run")
+        return ids, d2
+
+    def autotune(self, points, queries, reps=3, stream=None):
+        t = BatchTuning()
+        _check(lib().cukd_batch_autotune(self.h, _ptr(points), _ptr(queries.contiguous()), reps,
+                                         C.byref(t), _stream(stream)), "cukd_batch_autotune")
+        return t

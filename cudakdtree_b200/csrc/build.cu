@@ -38,8 +38,11 @@
 #include <atomic>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
+#include <vector>
 
 #include "common.cuh"
+#include "forest.cuh"
 
 namespace ckb {
 
@@ -66,6 +69,7 @@ void keep_default_pool_memory()
   doneMask[slot] |= bit;
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(long long d) { g_launches.fetch_add((unsigned long long)d, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(); }
 const char *last_cuda_error_string() { return cudaGetErrorString(g_last_cuda); }
 
@@ -240,7 +244,36 @@ struct LevelArgs {
   int chunksPerSeg;
   int nseg;
   int cb;  // current key buffer
+  // forest builds (many trees in one array): per work item its cloud, its
+  // subtree's index on the level and its first child's work item in the next
+  // level (-1: the children are finished by the subtree phase); per cloud its
+  // first record and record count.  Null for a single tree.
+  const int32_t *wCloud, *wLocal, *wChild;
+  const int64_t *cBase, *cN;
 };
+
+// subtree handled by work item w: tree size, node id, the tree's first
+// record in the working arrays, and the children's work item
+struct SegGeo {
+  int64_t n, g, base, child;
+};
+__device__ inline SegGeo seg_geo(const LevelArgs &a, int w)
+{
+  SegGeo s;
+  if (a.wCloud) {
+    const int c = a.wCloud[w];
+    s.n = a.cN[c];
+    s.base = a.cBase[c];
+    s.g = ((int64_t(1) << a.level) - 1) + a.wLocal[w];
+    s.child = a.wChild[w];
+  } else {
+    s.n = a.n;
+    s.base = 0;
+    s.g = ((int64_t(1) << a.level) - 1) + w;
+    s.child = 2 * int64_t(w);
+  }
+  return s;
+}
 
 template <int SC, int D>
 __global__ void __launch_bounds__(kGThreads) hist_kernel(Bufs b, LevelArgs a)
@@ -248,9 +281,9 @@ __global__ void __launch_bounds__(kGThreads) hist_kernel(Bufs b, LevelArgs a)
   __shared__ uint32_t sh[kMaxBins];
   const int seg = blockIdx.x / a.chunksPerSeg;
   const int chunk = blockIdx.x % a.chunksPerSeg;
-  const int64_t g = ((int64_t(1) << a.level) - 1) + seg;
-  const int64_t sb = seg_begin(g, a.level, a.n);
-  const int64_t sz = subtree_size(g, a.n);
+  const SegGeo sg = seg_geo(a, seg);
+  const int64_t sb = sg.base + seg_begin(sg.g, a.level, sg.n);
+  const int64_t sz = subtree_size(sg.g, sg.n);
   const int64_t c0 = int64_t(chunk) * kChunk;
   if (c0 >= sz) return;
   const int64_t c1 = min(sz, c0 + kChunk);
@@ -272,8 +305,8 @@ __global__ void select_kernel(Bufs b, LevelArgs a)
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= a.nseg) return;
-  const int64_t g = ((int64_t(1) << a.level) - 1) + warp;
-  const uint32_t r = uint32_t(left_size(g, a.n));
+  const SegGeo sg = seg_geo(a, warp);
+  const uint32_t r = uint32_t(left_size(sg.g, sg.n));
   const uint32_t *h = b.hist + int64_t(warp) * a.nb;
   const int per = a.nb / 32;
   uint32_t s = 0;
@@ -305,6 +338,7 @@ template <int D>
 __device__ inline void merge_child_bounds(uint32_t (&lo)[2][D], uint32_t (&hi)[2][D],
                                           uint32_t *bmin, uint32_t *bmax, int64_t childIdx)
 {
+  if (childIdx < 0) return;  // children finished by the subtree phase
 #pragma unroll
   for (int s = 0; s < 2; s++)
 #pragma unroll
@@ -330,9 +364,10 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
   __shared__ uint32_t base[3];
   const int seg = blockIdx.x / a.chunksPerSeg;
   const int chunk = blockIdx.x % a.chunksPerSeg;
-  const int64_t g = ((int64_t(1) << a.level) - 1) + seg;
-  const int64_t sb = seg_begin(g, a.level, a.n);
-  const int64_t sz = subtree_size(g, a.n);
+  const SegGeo sg = seg_geo(a, seg);
+  const int64_t g = sg.g;
+  const int64_t sb = sg.base + seg_begin(g, a.level, sg.n);
+  const int64_t sz = subtree_size(g, sg.n);
   const int64_t c0 = int64_t(chunk) * kChunk;
   if (c0 >= sz) return;
   const int64_t c1 = min(sz, c0 + kChunk);
@@ -385,8 +420,8 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
 
   const int64_t lchild = 2 * g + 1;
   const int lvlNext = a.level + 1;
-  const int64_t lBeg = seg_begin(lchild, lvlNext, a.n);
-  const int64_t rBeg = seg_begin(lchild + 1, lvlNext, a.n);
+  const int64_t lBeg = sg.base + seg_begin(lchild, lvlNext, sg.n);
+  const int64_t rBeg = sg.base + seg_begin(lchild + 1, lvlNext, sg.n);
   uint32_t lo[2][D], hi[2][D];
 #pragma unroll
   for (int s = 0; s < 2; s++)
@@ -421,7 +456,7 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
       }
     }
   }
-  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], 2 * int64_t(seg));
+  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
 }
 
 // MSD radix select on the composite key among a subtree's candidates, then
@@ -434,12 +469,13 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
   __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr;
   __shared__ uint32_t pw[D + 1];
   const int seg = blockIdx.x;
-  const int64_t g = ((int64_t(1) << a.level) - 1) + seg;
-  const int64_t sb = seg_begin(g, a.level, a.n);
-  const int64_t sz = subtree_size(g, a.n);
+  const SegGeo sg = seg_geo(a, seg);
+  const int64_t g = sg.g;
+  const int64_t sb = sg.base + seg_begin(g, a.level, sg.n);
+  const int64_t sz = subtree_size(g, sg.n);
   const uint32_t below = b.sel[seg * 3 + 1];
   const uint32_t m = b.sel[seg * 3 + 2];
-  const uint32_t r = uint32_t(left_size(g, a.n));
+  const uint32_t r = uint32_t(left_size(g, sg.n));
   const int dim = b.sdim[0][seg];
 
   // composite order: own dim, then ancestors' dims nearest first, then index
@@ -448,7 +484,7 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
   cd[ncd++] = dim;
   for (int64_t an = g; an > 0 && ncd < D;) {
     an = (an - 1) >> 1;
-    const int da = explicitDims ? int(b.ndim[an]) : rr_dim(an, D);
+    const int da = explicitDims ? int(b.ndim[sg.base + an]) : rr_dim(an, D);
     bool seen = false;
     for (int i = 0; i < ncd; i++) seen |= (cd[i] == da);
     if (!seen) cd[ncd++] = da;
@@ -542,8 +578,8 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
 
   const int64_t lchild = 2 * g + 1;
   const int lvlNext = a.level + 1;
-  const int64_t lBeg = seg_begin(lchild, lvlNext, a.n) + below;
-  const int64_t rBeg = seg_begin(lchild + 1, lvlNext, a.n) + (uint32_t(sz) - m - below);
+  const int64_t lBeg = sg.base + seg_begin(lchild, lvlNext, sg.n) + below;
+  const int64_t rBeg = sg.base + seg_begin(lchild + 1, lvlNext, sg.n) + (uint32_t(sz) - m - below);
   const int nbuf = a.cb ^ 1;
   uint32_t lo[2][D], hi[2][D];
 #pragma unroll
@@ -575,10 +611,12 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
       b.idx[nbuf][dst] = b.cidx[sb + i];
     }
   }
-  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], 2 * int64_t(seg));
+  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
   if (threadIdx.x == 0) {
-    b.perm[g] = b.cidx[sb + piv];
-    b.ndim[g] = uint8_t(dim);
+    b.perm[sg.base + g] = b.cidx[sb + piv];
+    b.ndim[sg.base + g] = uint8_t(dim);
+  }
+  if (threadIdx.x == 0 && sg.child >= 0) {
     uint32_t bl[D], bh[D];
     for (int d = 0; d < D; d++) {
       bl[d] = b.sbox[0][int64_t(seg) * 2 * D + d];
@@ -594,7 +632,7 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
         ch[dim] = pkey[dim];
       else
         cl[dim] = pkey[dim];
-      const int64_t ci = 2 * int64_t(seg) + s;
+      const int64_t ci = sg.child + s;
       for (int d = 0; d < D; d++) {
         b.sbox[1][ci * 2 * D + d] = cl[d];
         b.sbox[1][ci * 2 * D + D + d] = ch[d];
@@ -608,39 +646,38 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
 // ---------------------------------------------------------------------------
 // subtree phase: one CTA per subtree of <= kTile points
 // ---------------------------------------------------------------------------
-template <int D>
+template <int D, int TILE>
 struct SubSmem {
-  uint32_t key[D][kTile];
-  uint32_t idx[kTile];
-  uint16_t list[2][D][kTile];
-  uint16_t segOf[2][kTile];
-  uint32_t scan[kTile];
+  uint32_t key[D][TILE];
+  uint32_t idx[TILE];
+  uint16_t list[2][D][TILE];
+  uint16_t segOf[2][TILE];
+  uint32_t scan[TILE];
   union {
-    unsigned long long sortbuf[kTile];
+    unsigned long long sortbuf[TILE];
     struct {
-      uint16_t t0[kTile], t1[kTile], b[kTile], r[kTile];
+      uint16_t t0[TILE], t1[TILE], b[TILE], r[TILE];
     } sub;
   } u;
-  uint16_t locPivot[2 * kTile];
-  uint8_t locDim[2 * kTile];
-  uint8_t flag[kTile];
-  uint8_t subDim[kTile];
-  uint16_t queue[kTile];
+  uint16_t locPivot[2 * TILE];
+  uint8_t locDim[2 * TILE];
+  uint8_t flag[TILE];
+  uint8_t subDim[TILE];
+  uint16_t queue[TILE];
   uint32_t warpSums[kSubThreads / 32];
   uint32_t qcount;
   uint32_t rootLo[D], rootHi[D];
 };
 
-template <int SC, int D>
-__global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
-                                                              bool explicitDims)
+// Finishes the subtree under node s (level L0) of a tree of n records whose
+// first record sits at `base` of the working arrays; `boxIndex` selects the
+// subtree's domain box in b.sbox[0] (explicit dims only).
+template <int SC, int D, int TILE>
+__device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_t base,
+                             int64_t boxIndex, int cb, bool explicitDims, SubSmem<D, TILE> &S)
 {
-  extern __shared__ __align__(16) uint8_t smem_raw[];
-  SubSmem<D> &S = *reinterpret_cast<SubSmem<D> *>(smem_raw);
   const int tid = threadIdx.x;
-  const int seg = blockIdx.x;
-  const int64_t s = ((int64_t(1) << L0) - 1) + seg;
-  const int64_t sb = seg_begin(s, L0, n);
+  const int64_t sb = base + seg_begin(s, L0, n);
   const int m = int(subtree_size(s, n));
   if (m == 0) return;
 
@@ -650,9 +687,9 @@ __global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n,
     S.idx[i] = b.idx[cb][sb + i];
     S.segOf[0][i] = 0;
   }
-  if (tid < D) {
-    S.rootLo[tid] = b.sbox[0][int64_t(seg) * 2 * D + tid];
-    S.rootHi[tid] = b.sbox[0][int64_t(seg) * 2 * D + D + tid];
+  if (tid < D && boxIndex >= 0) {
+    S.rootLo[tid] = b.sbox[0][boxIndex * 2 * D + tid];
+    S.rootHi[tid] = b.sbox[0][boxIndex * 2 * D + D + tid];
   }
   __syncthreads();
 
@@ -758,8 +795,8 @@ __global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n,
         const int piv = Ld[pp];
         S.flag[piv] = 2;
         S.locPivot[u] = uint16_t(piv);
-        b.perm[g] = S.idx[piv];
-        b.ndim[g] = uint8_t(dim);
+        b.perm[base + g] = S.idx[piv];
+        b.ndim[base + g] = uint8_t(dim);
       } else {
         S.queue[atomicAdd(&S.qcount, 1u)] = uint16_t(t);
       }
@@ -785,7 +822,7 @@ __global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n,
             c = (c - 1) >> 1;
             da = S.locDim[c];
           } else {
-            da = explicitDims ? int(b.ndim[(ga - 1) >> 1]) : rr_dim((ga - 1) >> 1, D);
+            da = explicitDims ? int(b.ndim[base + ((ga - 1) >> 1)]) : rr_dim((ga - 1) >> 1, D);
           }
           ga = (ga - 1) >> 1;
           bool seen = false;
@@ -819,8 +856,8 @@ __global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n,
         else {
           S.flag[ex] = 2;
           S.locPivot[u] = uint16_t(ex);
-          b.perm[g] = S.idx[ex];
-          b.ndim[g] = uint8_t(dim);
+          b.perm[base + g] = S.idx[ex];
+          b.ndim[base + g] = uint8_t(dim);
         }
       }
     }
@@ -836,7 +873,7 @@ __global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n,
     }
     __syncthreads();
     // C: stable partition of every list (pivots dropped)
-    constexpr int PER = kTile / kSubThreads;
+    constexpr int PER = TILE / kSubThreads;
     for (int d = 0; d < D; d++) {
       const uint16_t *Lc = S.list[cur][d];
       uint32_t local = 0;
@@ -886,6 +923,41 @@ __global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n,
     }
     mact -= nexist;
     cur ^= 1;
+  }
+}
+
+template <int SC, int D>
+__global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
+                                                              bool explicitDims)
+{
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  SubSmem<D, kTile> &S = *reinterpret_cast<SubSmem<D, kTile> *>(smem_raw);
+  const int seg = blockIdx.x;
+  subtree_body<SC, D, kTile>(b, n, L0, ((int64_t(1) << L0) - 1) + seg, 0, seg, cb, explicitDims,
+                             S);
+}
+
+// Forest subtree phase, persistent: each CTA takes the next (tree, subtree)
+// work item from a global counter until the list (sorted by size, largest
+// first) is exhausted.  A tree whose top-down phase ran L0 levels left its
+// records in key buffer L0 & 1.  Round-robin split dims.
+template <int D, int TILE>
+__global__ void __launch_bounds__(kSubThreads) subtree_forest_kernel(Bufs b, ForestSubtrees f)
+{
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  SubSmem<D, TILE> &S = *reinterpret_cast<SubSmem<D, TILE> *>(smem_raw);
+  __shared__ int next;
+  for (;;) {
+    if (threadIdx.x == 0) next = atomicAdd(f.counter, 1);
+    __syncthreads();
+    const int w = next;
+    __syncthreads();
+    if (w >= f.items) break;
+    const int c = f.cloud[w];
+    const int L0 = f.level[w];
+    subtree_body<0, D, TILE>(b, f.cloudN[c], L0, ((int64_t(1) << L0) - 1) + f.local[w],
+                             f.cloudBase[c], -1, L0 & 1, false, S);
+    __syncthreads();
   }
 }
 
@@ -980,7 +1052,7 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
   for (int lvl = 0; lvl < G; lvl++) {
     const int nseg = 1 << lvl;
     const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
-    LevelArgs a;
+    LevelArgs a{};
     a.n = n;
     a.level = lvl;
     a.nb = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
@@ -1006,7 +1078,7 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
     std::swap(b.sbox[0], b.sbox[1]);
   }
   {
-    const size_t smem = sizeof(SubSmem<D>);
+    const size_t smem = sizeof(SubSmem<D, kTile>);
     CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
@@ -1199,7 +1271,7 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
   for (int lvl = 0; lvl < G; lvl++) {
     const int nseg = 1 << lvl;
     const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
-    LevelArgs a;
+    LevelArgs a{};
     a.n = n;
     a.level = lvl;
     a.nb = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
@@ -1225,7 +1297,7 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
     std::swap(b.sbox[0], b.sbox[1]);
   }
   {
-    const size_t smem = sizeof(SubSmem<D>);
+    const size_t smem = sizeof(SubSmem<D, kTile>);
     CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
@@ -1241,7 +1313,272 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
   return CUKD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// forest builds (many clouds in one record array)
+// ---------------------------------------------------------------------------
+// Per cloud: its data bounds (one CTA per cloud over the extracted keys),
+// the root state of clouds that start with top-down levels, and the float
+// box output (lower[D] then upper[D]; an empty cloud gets +inf / -inf).
+template <int D>
+__global__ void __launch_bounds__(256) cloud_bounds_kernel(Bufs b, const int64_t *cBase,
+                                                           const int64_t *cN,
+                                                           const int32_t *rootItem,
+                                                           float *boundsOut)
+{
+  __shared__ uint32_t sl[8][D], sh[8][D];
+  const int c = blockIdx.x;
+  const int64_t base = cBase[c], n = cN[c];
+  uint32_t lo[D], hi[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    lo[d] = 0xffffffffu;
+    hi[d] = 0u;
+  }
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const uint32_t k = b.key[0][d][base + i];
+      lo[d] = min(lo[d], k);
+      hi[d] = max(hi[d], k);
+    }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = min(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = max(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+    if (lane == 0) {
+      sl[wid][d] = lo[d];
+      sh[wid][d] = hi[d];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (int w = 1; w < int(blockDim.x >> 5); w++)
+    for (int d = 0; d < D; d++) {
+      lo[d] = min(lo[d], sl[w][d]);
+      hi[d] = max(hi[d], sh[w][d]);
+    }
+  if (boundsOut) {
+    float *o = boundsOut + int64_t(c) * 2 * D;
+    for (int d = 0; d < D; d++) {
+      o[d] = n > 0 ? key_float(lo[d]) : __int_as_float(0x7f800000);
+      o[D + d] = n > 0 ? key_float(hi[d]) : __int_as_float(0xff800000);
+    }
+  }
+  const int it = rootItem[c];
+  if (it >= 0) {
+    for (int d = 0; d < D; d++) {
+      b.sbmin[0][int64_t(it) * D + d] = lo[d];
+      b.sbmax[0][int64_t(it) * D + d] = hi[d];
+      b.sbox[0][int64_t(it) * 2 * D + d] = lo[d];
+      b.sbox[0][int64_t(it) * 2 * D + D + d] = hi[d];
+    }
+    b.sdim[0][it] = 0;
+  }
+}
+
+struct ForestWs {
+  Bufs b;
+  uint8_t *orig;
+  std::vector<void *> blocks;
+};
+
+template <int D>
+int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaStream_t st,
+                      cudaStream_t side[3], cudaEvent_t ev[4])
+{
+  ForestWs *ws = (ForestWs *)f.ws;
+  if (!ws) return CUKD_ERR_INVALID_ARGUMENT;
+  Bufs b = ws->b;
+  const int64_t n = f.total;
+  const int stride = 4 * D;
+  if (n == 0) return CUKD_OK;
+  CKB_CUDA(cudaMemsetAsync(b.wbmin, 0xff, sizeof(uint32_t) * D, st));
+  CKB_CUDA(cudaMemsetAsync(b.wbmax, 0, sizeof(uint32_t) * D, st));
+  {
+    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 8));
+    extract_kernel<0, D><<<blocks, 256, 0, st>>>((const uint8_t *)pts, n, stride, 0, ws->orig, b);
+    CKB_CHECK_LAUNCH();
+  }
+  cloud_bounds_kernel<D><<<unsigned(f.numClouds), 256, 0, st>>>(b, f.cloudBase, f.cloudN,
+                                                                f.rootItem, boundsOut);
+  CKB_CHECK_LAUNCH();
+  int cb = 0;
+  for (int lvl = 0; lvl < f.numLevels; lvl++) {
+    const ForestLevel &L = f.level[lvl];
+    const int nextItems = lvl + 1 < f.numLevels ? f.level[lvl + 1].items : 0;
+    LevelArgs a{};
+    a.n = 0;
+    a.level = lvl;
+    a.nb = L.nb;
+    a.chunksPerSeg = L.chunksPerSeg;
+    a.nseg = L.items;
+    a.cb = cb;
+    a.wCloud = L.cloud;
+    a.wLocal = L.local;
+    a.wChild = L.child;
+    a.cBase = f.cloudBase;
+    a.cN = f.cloudN;
+    CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(L.items) * L.nb, st));
+    if (nextItems > 0) {
+      CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * size_t(nextItems) * D, st));
+      CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * size_t(nextItems) * D, st));
+    }
+    const int64_t grid = int64_t(L.items) * L.chunksPerSeg;
+    hist_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    select_kernel<<<unsigned(div_up(int64_t(L.items) * 32, 256)), 256, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    partition_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    CKB_CHECK_LAUNCH();
+    resolve_kernel<0, D><<<unsigned(L.items), kGThreads, 0, st>>>(b, a, false);
+    CKB_CHECK_LAUNCH();
+    cb ^= 1;
+    std::swap(b.sdim[0], b.sdim[1]);
+    std::swap(b.sbmin[0], b.sbmin[1]);
+    std::swap(b.sbmax[0], b.sbmax[1]);
+    std::swap(b.sbox[0], b.sbox[1]);
+  }
+  // subtree phase: one persistent launch per tile class; with side streams
+  // the classes are concurrent branches (fork / join through events)
+  const bool fork = side && ev;
+  if (fork) CKB_CUDA(cudaEventRecord(ev[3], st));
+  for (int c = 0; c < 3; c++) {
+    const ForestSubtrees &S = f.sub[c];
+    if (S.items == 0) continue;
+    cudaStream_t s = st;
+    if (fork) {
+      s = side[c];
+      CKB_CUDA(cudaStreamWaitEvent(s, ev[3], 0));
+    }
+    CKB_CUDA(cudaMemsetAsync(S.counter, 0, sizeof(int), s));
+    const int grid = std::max(1, std::min(S.items, f.subGrid[c]));
+    // (the shared-memory opt-in was made by forest_subtree_occupancy)
+#define CKB_SUB(T_)                                                                 \
+  if (kForestTiles[c] == T_) {                                                      \
+    subtree_forest_kernel<D, T_><<<grid, kSubThreads, sizeof(SubSmem<D, T_>), s>>>(b, S); \
+    CKB_CHECK_LAUNCH();                                                             \
+  }
+    CKB_SUB(512) CKB_SUB(1024) CKB_SUB(2048)
+#undef CKB_SUB
+    if (fork) {
+      CKB_CUDA(cudaEventRecord(ev[c], s));
+      CKB_CUDA(cudaStreamWaitEvent(st, ev[c], 0));
+    }
+  }
+  {
+    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 16));
+    finalize_kernel<<<blocks, 256, 0, st>>>((uint8_t *)pts, ws->orig, b.perm, b.ndim, n, stride,
+                                            -1, 0, 0u);
+    CKB_CHECK_LAUNCH();
+  }
+  return CUKD_OK;
+}
+
+template <int D, int T>
+int subtree_occupancy()
+{
+  int blocks = 0;
+  const size_t smem = sizeof(SubSmem<D, T>);
+  if (cudaFuncSetAttribute(subtree_forest_kernel<D, T>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, subtree_forest_kernel<D, T>,
+                                                    kSubThreads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  return std::max(1, blocks);
+}
+
 }  // namespace build
+
+int forest_workspace_create(ForestBuild *f, int64_t maxItems, int64_t histCap)
+{
+  using namespace build;
+  if (!f || f->D < 2 || f->D > 4) return CUKD_ERR_INVALID_ARGUMENT;
+  forest_workspace_destroy(f);
+  ForestWs *ws = new ForestWs();
+  ws->b = Bufs{};
+  const int D = f->D;
+  const int64_t n = std::max<int64_t>(f->total, 1);
+  const int64_t items = std::max<int64_t>(maxItems, 1);
+  auto get = [&](auto **out, size_t count) -> int {
+    void *p = nullptr;
+    const size_t bytes = std::max<size_t>(16, count * sizeof(**out));
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return CUKD_ERR_OUT_OF_MEMORY;
+    }
+    ws->blocks.push_back(p);
+    *out = (std::remove_reference_t<decltype(**out)> *)p;
+    return CUKD_OK;
+  };
+  int rc = CUKD_OK;
+  auto T = [&](int r) {
+    if (rc == CUKD_OK) rc = r;
+  };
+  Bufs &b = ws->b;
+  for (int x = 0; x < 2; x++) {
+    for (int d = 0; d < D; d++) T(get(&b.key[x][d], n));
+    T(get(&b.idx[x], n));
+  }
+  if (maxItems > 0) {
+    for (int d = 0; d < D; d++) T(get(&b.ckey[d], n));
+    T(get(&b.cidx, n));
+  }
+  T(get(&b.perm, n));
+  T(get(&b.ndim, n));
+  T(get(&ws->orig, size_t(n) * 4 * D));
+  for (int x = 0; x < 2; x++) {
+    T(get(&b.sdim[x], items));
+    T(get(&b.sbmin[x], items * D));
+    T(get(&b.sbmax[x], items * D));
+    T(get(&b.sbox[x], items * 2 * D));
+  }
+  T(get(&b.hist, std::max<int64_t>(histCap, 64)));
+  T(get(&b.sel, items * 3));
+  T(get(&b.cur, items * 3));
+  T(get(&b.wbmin, D));
+  T(get(&b.wbmax, D));
+  f->ws = ws;
+  if (rc != CUKD_OK) forest_workspace_destroy(f);
+  return rc;
+}
+
+void forest_workspace_destroy(ForestBuild *f)
+{
+  if (!f || !f->ws) return;
+  build::ForestWs *ws = (build::ForestWs *)f->ws;
+  for (void *p : ws->blocks) cudaFree(p);
+  delete ws;
+  f->ws = nullptr;
+}
+
+int forest_subtree_occupancy(int D, int c)
+{
+  using namespace build;
+#define CKB_OCC(D_)                                          \
+  if (D == D_) {                                             \
+    if (c == 0) return subtree_occupancy<D_, 512>();         \
+    if (c == 1) return subtree_occupancy<D_, 1024>();        \
+    return subtree_occupancy<D_, 2048>();                    \
+  }
+  CKB_OCC(2) CKB_OCC(3) CKB_OCC(4)
+#undef CKB_OCC
+  return 1;
+}
+
+int forest_build(const ForestBuild &f, float *pts, float *boundsOut, cudaStream_t st,
+                 cudaStream_t side[3], cudaEvent_t ev[4])
+{
+  using namespace build;
+  if (f.D == 2) return forest_build_impl<2>(f, pts, boundsOut, st, side, ev);
+  if (f.D == 3) return forest_build_impl<3>(f, pts, boundsOut, st, side, ev);
+  if (f.D == 4) return forest_build_impl<4>(f, pts, boundsOut, st, side, ev);
+  return CUKD_ERR_UNSUPPORTED;
+}
 
 int build_dispatch(void *pts, int64_t n, const Layout &L, void *wb, cudaStream_t st,
                    const cukd_mem_resource *mem)

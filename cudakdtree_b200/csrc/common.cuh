@@ -17,6 +17,10 @@ namespace ckb {
 void set_cuda_error(cudaError_t e);
 // number of kernels this library has launched (reported by the benchmark)
 void count_launch();
+// adjusts the count: + kernels a replayed CUDA graph launched, - kernels
+// that were only recorded into a graph
+void add_launches(long long d);
+unsigned long long launch_count();
 
 #define CKB_CHECK_LAUNCH()                           \
   do {                                               \

@@ -37,6 +37,7 @@ namespace ckb {
 namespace fast {
 
 using query::QArgs;
+using query::TreeView;
 
 // One thread per query (queries in Morton order).  Culling uses the
 // closest-corner distance of each subtree's domain box, the bound of
@@ -47,16 +48,14 @@ using query::QArgs;
 // difference of a smaller magnitude), so "<=" culling sees every point with
 // d2 <= the final (k+1)-th distance.
 template <int D, bool EXPL, bool VEC16, int KC>
-__global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
+__device__ __forceinline__ void knn_fast_one(const FastArgs &fa, int64_t i)
 {
   const QArgs &a = fa.q;
-  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  const int64_t limit = a.count_ptr ? int64_t(*a.count_ptr) : a.nq;
-  if (i >= limit) return;
   const int64_t myq = a.order ? int64_t(a.order[i]) : i;
-  const int N = int(a.n);
+  const TreeView tv = query::tree_of<D, 4>(a, myq);
+  const int N = int(tv.n);
   const int k = fa.kk;  // live slots: k+1, right-aligned
-  const uint8_t *tree = a.tree;
+  const uint8_t *tree = tv.tree;
 
   float q[D];
   {
@@ -84,7 +83,7 @@ __global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
 
   // closest point of the root's box (the world bounds, or all of space)
   float closest[D];
-  const float *bnd = (const float *)a.bounds;
+  const float *bnd = (const float *)tv.bounds;
 #pragma unroll
   for (int d = 0; d < D; d++) {
     float v = q[d];
@@ -244,10 +243,21 @@ __global__ void __launch_bounds__(128) knn_fast_kernel(FastArgs fa)
 }
 
 template <int D, bool EXPL, bool VEC16, int KC>
+__global__ void __launch_bounds__(256) knn_fast_kernel(FastArgs fa)
+{
+  const int64_t limit = fa.q.count_ptr ? int64_t(*fa.q.count_ptr) : fa.q.nq;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < limit;
+       i += int64_t(gridDim.x) * blockDim.x)
+    knn_fast_one<D, EXPL, VEC16, KC>(fa, i);
+}
+
+template <int D, bool EXPL, bool VEC16, int KC>
 int launch_fast(const FastArgs &fa, cudaStream_t st)
 {
   const int bs = fa.q.block_size > 0 ? fa.q.block_size : 128;
-  knn_fast_kernel<D, EXPL, VEC16, KC><<<unsigned(div_up(fa.q.nq, bs)), bs, 0, st>>>(fa);
+  const int qpt = fa.q.queries_per_thread > 1 ? fa.q.queries_per_thread : 1;
+  const int64_t grid = std::max<int64_t>(1, div_up(fa.q.nq, int64_t(bs) * qpt));
+  knn_fast_kernel<D, EXPL, VEC16, KC><<<unsigned(grid), bs, 0, st>>>(fa);
   CKB_CHECK_LAUNCH();
   return CUKD_OK;
 }

@@ -28,7 +28,7 @@ namespace query {
 // kernels
 // ---------------------------------------------------------------------------
 template <int SC, int D, bool EXPL, bool VEC16, int METHOD, class Res>
-__global__ void __launch_bounds__(128) query_kernel(QArgs a)
+__global__ void __launch_bounds__(256) query_kernel(QArgs a)
 {
   using Tr = Traits<SC>;
   using T = typename Tr::T;
@@ -40,14 +40,16 @@ __global__ void __launch_bounds__(128) query_kernel(QArgs a)
     const T *qp = (const T *)a.queries + qi * D;
 #pragma unroll
     for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
+    const TreeView tv = tree_of<D, sizeof(T)>(a, qi);
     NodeReader<SC, D, EXPL, VEC16> rd(a);
+    rd.tree = tv.tree;
     Res res(a);
     if (METHOD == CUKD_STACK_BASED)
-      trav_stack_based<SC, D>(res, q, rd, a.n);
+      trav_stack_based<SC, D>(res, q, rd, tv.n);
     else if (METHOD == CUKD_STACK_FREE)
-      trav_stack_free<SC, D>(res, q, rd, a.n, a.eps);
+      trav_stack_free<SC, D>(res, q, rd, tv.n, a.eps);
     else
-      trav_cct<SC, D>(res, q, rd, a.n, (const T *)a.bounds);
+      trav_cct<SC, D>(res, q, rd, tv.n, (const T *)tv.bounds);
     res.write(a, qi);
   }
 }
@@ -132,6 +134,8 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   if (!d_queries || (!ids && !visits) || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;
   if (p->method < CUKD_STACK_BASED || p->method > CUKD_CCT) return CUKD_ERR_INVALID_ARGUMENT;
   if (p->method == CUKD_CCT && !d_world_bounds) return CUKD_ERR_INVALID_ARGUMENT;
+  if (p->block_size != 0 && (p->block_size < 32 || p->block_size > 256 || p->block_size % 32))
+    return CUKD_ERR_INVALID_ARGUMENT;
   int kind = RES_FCP;
   if (knn) {
     const int k = p->k;

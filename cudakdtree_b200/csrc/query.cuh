@@ -30,7 +30,36 @@ struct QArgs {
   int32_t *flags_out;   // optional per-query status (learned path)
   int block_size;
   const int *count_ptr;  // optional device-side number of queries in `order`
+  // forest (batched clouds): when q_cloud is set, query i searches the tree
+  // of cloud q_cloud[i], records [cloud_base[c], cloud_base[c + 1]) of
+  // `tree`, whose box is cloud_bounds[c] (lower[D], upper[D]; optional);
+  // the ids are local to that cloud
+  const int32_t *q_cloud;
+  const int64_t *cloud_base;
+  const void *cloud_bounds;
+  int queries_per_thread;  // fast kernel: queries a thread runs in turn
 };
+
+// the tree a query searches: the whole tree, or its cloud's (forest)
+struct TreeView {
+  const uint8_t *tree;
+  int64_t n;
+  const void *bounds;
+};
+template <int D, int BYTES>
+__device__ __forceinline__ TreeView tree_of(const QArgs &a, int64_t qi)
+{
+  TreeView t{a.tree, a.n, a.bounds};
+  if (a.q_cloud) {
+    const int c = __ldg(a.q_cloud + qi);
+    const int64_t b0 = __ldg((const long long *)a.cloud_base + c);
+    t.n = __ldg((const long long *)a.cloud_base + c + 1) - b0;
+    t.tree = a.tree + b0 * a.stride;
+    t.bounds = a.cloud_bounds ? (const uint8_t *)a.cloud_bounds + int64_t(c) * 2 * D * BYTES
+                              : nullptr;
+  }
+  return t;
+}
 
 enum { RES_FCP = 0, RES_FIX4, RES_FIX8, RES_FIX16, RES_FIX32, RES_HEAP128, RES_HEAP1024 };
 

@@ -111,13 +111,22 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(
 
 }  // namespace
 
+int64_t radix_sort_counts(int64_t n) { return std::max<int64_t>(1, div_up(n, kTileItems)) * 256; }
+
 int radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys2, uint32_t *vals2,
                      int64_t n, int bits, cudaStream_t st, TempArena *arena)
 {
   if (n <= 1 || bits <= 0) return CUKD_OK;
-  const int numTiles = int(div_up(n, kTileItems));
   uint32_t *counts = nullptr;
-  CKB_TRY(arena->alloc(&counts, size_t(numTiles) * 256));
+  CKB_TRY(arena->alloc(&counts, size_t(radix_sort_counts(n))));
+  return radix_sort_pairs_ws(keys, vals, keys2, vals2, n, bits, counts, st);
+}
+
+int radix_sort_pairs_ws(uint32_t *keys, uint32_t *vals, uint32_t *keys2, uint32_t *vals2,
+                        int64_t n, int bits, uint32_t *counts, cudaStream_t st)
+{
+  if (n <= 1 || bits <= 0) return CUKD_OK;
+  const int numTiles = int(div_up(n, kTileItems));
   uint32_t *ka = keys, *va = vals, *kb = keys2, *vb = vals2;
   int passes = 0;
   for (int shift = 0; shift < bits; shift += 8, passes++) {

@@ -10,4 +10,10 @@ namespace ckb {
 int radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys2, uint32_t *vals2,
                      int64_t n, int bits, cudaStream_t st, TempArena *arena);
 
+// Same with caller-provided scratch of radix_sort_counts(n) entries (no
+// allocation: usable inside CUDA graph capture).
+int64_t radix_sort_counts(int64_t n);
+int radix_sort_pairs_ws(uint32_t *keys, uint32_t *vals, uint32_t *keys2, uint32_t *vals2,
+                        int64_t n, int bits, uint32_t *counts, cudaStream_t st);
+
 }  // namespace ckb

@@ -189,7 +189,7 @@ typedef struct cukd_query_params {
   float eps;             /* FcpSearchParams::eps, honoured by CUKD_STACK_FREE */
   int64_t cutoff_d2;     /* int trees: squared cut-off radius (INT64_MAX = none) */
   int32_t flags;         /* CUKD_QUERY_* */
-  int32_t block_size;    /* 0 = default; else threads per block (autotuner) */
+  int32_t block_size;    /* 0 = default (128); else threads per block, 32..256 */
   /* optional device int: receives how many queries were re-run in the
    * reference's visiting order (distance ties at the k-th boundary) */
   int32_t *d_reordered_count;
@@ -344,6 +344,69 @@ CUKD_API int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *
                               float radius_scale, int32_t *d_out_ids, void *d_out_d2,
                               int32_t *d_out_fallback, int32_t *d_status, int64_t *d_visits,
                               cudaStream_t stream, const cukd_mem_resource *mem);
+
+/* ------------------------------------------------------------------------
+ * Batched clouds (no reference counterpart: the reference builds and
+ * queries one tree per call, cukd/builder.h:108-122, and its samples loop
+ * over calls)
+ *
+ * B independent float clouds (num_dims = 2..4) stored one after another in
+ * one array, with CSR offsets h_point_offsets[B + 1]; B query sets, CSR
+ * offsets h_query_offsets[B + 1], each answered against its own cloud.
+ * Every cloud becomes the same left-balanced tree (round-robin dims) that
+ * cukd_build_tree gives it alone, in place in its slice; query results are
+ * the per-cloud cukd_knn / cukd_fcp results with ids local to the cloud.
+ * The plan derives all per-level work lists from the sizes once and owns
+ * every temporary, so a run allocates nothing and a build + query can be
+ * recorded as one CUDA graph (cukd_batch_run) and replayed.
+ * ------------------------------------------------------------------------ */
+typedef struct cukd_batch_plan_s cukd_batch_plan;
+
+typedef struct cukd_batch_tuning {
+  int32_t build_tile;          /* subtree-phase tile: 512, 1024 or 2048 points */
+  int32_t block_size;          /* query threads per block: 32..256, multiple of 32 */
+  int32_t queries_per_thread;  /* 1, 2 or 4 */
+  int32_t morton;              /* 1: visit each cloud's queries in Morton order */
+  float build_ms, query_ms;    /* cukd_batch_autotune: best times measured */
+} cukd_batch_tuning;
+
+/* params: method, k (1..1024; 0 = FCP), cutoff_radius, eps, flags as for
+ * cukd_knn (CUKD_QUERY_MORTON is replaced by the tuning's `morton`).  The
+ * offsets are host arrays, non-decreasing, starting at 0.  Allocates the
+ * plan's device memory on the current device. */
+CUKD_API int cukd_batch_plan_create(cukd_batch_plan **out, int num_dims, int64_t num_clouds,
+                                    const int64_t *h_point_offsets,
+                                    const int64_t *h_query_offsets,
+                                    const cukd_query_params *params);
+CUKD_API int cukd_batch_plan_destroy(cukd_batch_plan *plan);
+CUKD_API int cukd_batch_get_tuning(const cukd_batch_plan *plan, cukd_batch_tuning *out);
+/* Validates and installs a tuning (drops a recorded graph). */
+CUKD_API int cukd_batch_set_tuning(cukd_batch_plan *plan, const cukd_batch_tuning *tuning);
+
+/* Builds every cloud of d_points (float[total][D]) in place; per-cloud
+ * boxes into d_cloud_bounds (optional, float[B][2][D]: lower then upper,
+ * +inf/-inf for an empty cloud). */
+CUKD_API int cukd_batch_build(cukd_batch_plan *plan, float *d_points, float *d_cloud_bounds,
+                              cudaStream_t stream);
+/* Queries of all clouds against built clouds: kNN writes d_out_ids /
+ * d_out_d2 as [nq][k], FCP as [nq] (d_out_d2 optional).  d_cloud_bounds
+ * (from cukd_batch_build) is required for CUKD_CCT and for Morton order. */
+CUKD_API int cukd_batch_query(cukd_batch_plan *plan, const float *d_points,
+                              const float *d_cloud_bounds, const float *d_queries,
+                              int32_t *d_out_ids, float *d_out_d2, cudaStream_t stream);
+/* Build + query as one CUDA graph: recorded on the first call with a set of
+ * pointers (and after a tuning change), replayed on the caller's stream
+ * afterwards.  d_cloud_bounds may be null (the plan keeps its own). */
+CUKD_API int cukd_batch_run(cukd_batch_plan *plan, float *d_points, float *d_cloud_bounds,
+                            const float *d_queries, int32_t *d_out_ids, float *d_out_d2,
+                            cudaStream_t stream);
+/* Times candidate tunings on the caller's data (build tiles, then query
+ * block size x queries per thread x Morton, `reps` runs each, median) and
+ * installs the fastest; d_points is copied, never modified.  *out
+ * (optional) receives the chosen tuning and its times.  Synchronises. */
+CUKD_API int cukd_batch_autotune(cukd_batch_plan *plan, const float *d_points,
+                                 const float *d_queries, int reps, cukd_batch_tuning *out,
+                                 cudaStream_t stream);
 
 /* ------------------------------------------------------------------------
  * Error strings
