@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -322,6 +323,8 @@ def run_ours(args, rank, world, local):
                "d2h_bytes_per_step": int(h_ids.numel() * 4 + h_d2.numel() * 4),
                "ms_per_step": round(et / args.steps, 3)}
 
+    batched = None if args.no_batched else batched_section(ck, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(d_pts.cpu().numpy(), wb.cpu().numpy(), q)
@@ -341,7 +344,7 @@ def run_ours(args, rank, world, local):
                          "knn_stack_based_reference_order": round(knn_ref_ms, 3)},
            "build_ms": round(build_ms, 3),
            "knn_stack_free_queries_per_s": round(nq / (knn_sf_ms / 1e3), 1),
-           "learned_radius": learned,
+           "learned_radius": learned, "batched": batched,
            "roofline": roofline, "build_roofline": build_roof,
            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
            "gpu_launches_per_step": round(launches / args.steps, 1)}
@@ -349,6 +352,59 @@ def run_ours(args, rank, world, local):
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def batched_section(ck, dev):
+    """Many clouds built and queried together (cukd_batch_*): 4096 clouds of
+    floor(exp(U[ln 256, ln 65536])) uniform points, 1024 uniform queries
+    each, k = 8, stack-based; autotuned, then timed as CUDA-graph replays
+    of build + query (the input cloud array is restored before each)."""
+    import torch
+    from cudakdtree_b200 import workloads as wl
+    pts, poff, qs, qoff = wl.batched_clouds()
+    plan = ck.BatchPlan(poff, qoff, 3, k=8)
+    src = torch.from_numpy(pts).to(dev)
+    P = torch.empty_like(src)
+    Q = torch.from_numpy(qs).to(dev)
+    bnd = plan.bounds_tensor(dev)
+    out = plan._outputs(dev)
+    tune = plan.autotune(src, Q, reps=3)
+
+    def run():
+        P.copy_(src, non_blocking=True)
+        plan.run(P, Q, bnd, out=out)
+
+    def timed(fn, reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    copy_ms = timed(lambda: P.copy_(src, non_blocking=True), 5)
+    l0 = ck.launch_count()
+    run_ms = timed(run, 10) - copy_ms
+    launches = (ck.launch_count() - l0) / 10
+    P.copy_(src)
+    build_ms = timed(lambda: (P.copy_(src, non_blocking=True), plan.build(P, bnd)), 5) - copy_ms
+    query_ms = timed(lambda: plan.query(P, Q, bnd, out=out), 5)
+    nq, n = qs.shape[0], pts.shape[0]
+    del plan
+    return {"workload": "4096 clouds, sizes floor(exp(U[ln 256, ln 65536])) (seed 5), uniform "
+                        "points and 1024 uniform queries per cloud, float3, k=8, stack_based",
+            "clouds": int(poff.size - 1), "points": int(n), "queries": int(nq), "k": 8,
+            "tuning": {k: (round(v, 3) if isinstance(v, float) else v)
+                       for k, v in tune.as_dict().items()},
+            "run_ms": round(run_ms, 3), "build_ms": round(build_ms, 3),
+            "query_ms": round(query_ms, 3),
+            "queries_per_s": round(nq / (run_ms / 1e3), 1),
+            "build_points_per_s": round(n / (build_ms / 1e3), 1),
+            "kernel_launches_per_run": launches, "graph": True}
 
 
 def cpu_baseline_sample(tree_records_i32, bounds, q):
