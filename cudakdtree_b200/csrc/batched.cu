@@ -63,6 +63,64 @@ __global__ void forest_morton_kernel(const float *__restrict__ q, int64_t nq, in
   }
 }
 
+// Per-cloud Morton order in shared memory: one CTA per cloud sorts its
+// queries' (code << 32 | local index) keys with a bitonic network and writes
+// the cloud's slice of the visiting order.  Needs <= kSegSortMax queries
+// per cloud (larger clouds take the global radix sort).
+constexpr int kSegSortMax = 8192;
+constexpr int kSegSortThreads = 512;
+
+__global__ void __launch_bounds__(kSegSortThreads) cloud_morton_sort_kernel(
+    const float *__restrict__ q, int D, const int64_t *__restrict__ qoff,
+    const float *__restrict__ cbounds, int32_t *order)
+{
+  extern __shared__ unsigned long long keys[];
+  const int c = blockIdx.x;
+  const int64_t b = qoff[c];
+  const int m = int(qoff[c + 1] - b);
+  if (m == 0) return;
+  int P = 1;
+  while (P < m) P <<= 1;
+  const int bits = 30 / D;
+  const float cells = float(1u << bits);
+  float lo[4], scale[4];
+  for (int d = 0; d < D; d++) {
+    const float l = cbounds[int64_t(c) * 2 * D + d], h = cbounds[int64_t(c) * 2 * D + D + d];
+    lo[d] = l;
+    scale[d] = h > l ? cells / (h - l) : 0.f;
+  }
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    unsigned long long k = ~0ull;
+    if (i < m) {
+      uint32_t code = 0;
+      for (int d = 0; d < D; d++) {
+        const float x = (q[(b + i) * D + d] - lo[d]) * scale[d];
+        const uint32_t cell = x >= 0.f ? (x < cells ? uint32_t(x) : (1u << bits) - 1u) : 0u;
+        for (int bb = 0; bb < bits; bb++) code |= ((cell >> bb) & 1u) << (bb * D + (D - 1 - d));
+      }
+      k = ((unsigned long long)code << 32) | uint32_t(i);
+    }
+    keys[i] = k;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
+        const int i = 2 * j * (t / j) + (t % j);
+        const int l = i + j;
+        const unsigned long long x = keys[i], y = keys[l];
+        const bool up = (i & k) == 0;
+        if ((x > y) == up) {
+          keys[i] = y;
+          keys[l] = x;
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    order[b + i] = int32_t(b + int64_t(uint32_t(keys[i])));
+}
+
 struct HostLists {
   int numLevels = 0;
   std::vector<int32_t> lvCloud[kForestMaxLevels], lvLocal[kForestMaxLevels],
@@ -182,6 +240,7 @@ struct cukd_batch_plan_s {
   uint32_t *mkeys = nullptr, *mvals = nullptr, *mkeys2 = nullptr, *mvals2 = nullptr;
   uint32_t *mcounts = nullptr;
   int32_t *fb_list = nullptr;
+  int64_t maxCloudQueries = 0;  // <= kSegSortMax: per-cloud Morton sort in shared memory
   int *ctr = nullptr;       // [0..1] fast-path counters, [2..4] subtree work counters
   void *lists = nullptr;    // current forest work lists (one block)
   float *tune_pts = nullptr;
@@ -342,7 +401,14 @@ static int query_impl(cukd_batch_plan_s *p, const float *pts, const float *bound
   int cloudBits = 0;
   while ((int64_t(1) << cloudBits) < p->B) cloudBits++;
   const int bits = std::min(10, (32 - cloudBits) / D);
-  if (p->tuning.morton && bounds && p->nq > 1 && bits >= 1) {
+  if (p->tuning.morton && bounds && p->nq > 1 && p->maxCloudQueries <= kSegSortMax) {
+    int P = 1;
+    while (P < p->maxCloudQueries) P <<= 1;
+    cloud_morton_sort_kernel<<<unsigned(p->B), kSegSortThreads, size_t(P) * 8, st>>>(
+        queries, D, p->d_qoff, bounds, (int32_t *)p->mvals);
+    CKB_CHECK_LAUNCH();
+    a.order = (const int32_t *)p->mvals;
+  } else if (p->tuning.morton && bounds && p->nq > 1 && bits >= 1) {
     const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(div_up(p->nq, 256), kNumSMs * 8)));
     forest_morton_kernel<<<blocks, 256, 0, st>>>(queries, p->nq, D, p->d_qcloud, bounds, bits,
                                                  p->mkeys, p->mvals);
@@ -490,6 +556,13 @@ int cukd_batch_plan_create(cukd_batch_plan **out, int num_dims, int64_t num_clou
     derive_lists(p->poff, kForestTiles[t], h);
     maxItems = std::max(maxItems, h.maxItems);
     histCap = std::max(histCap, h.histCap);
+  }
+  for (int64_t c = 0; c < B; c++)
+    p->maxCloudQueries = std::max(p->maxCloudQueries, p->qoff[c + 1] - p->qoff[c]);
+  if (cudaFuncSetAttribute(cloud_morton_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kSegSortMax * 8) != cudaSuccess) {
+    set_cuda_error(cudaGetLastError());
+    return fail(CUKD_ERR_CUDA);
   }
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);

@@ -355,13 +355,19 @@ __device__ inline void merge_child_bounds(uint32_t (&lo)[2][D], uint32_t (&hi)[2
     }
 }
 
+// Each warp owns a contiguous run of kChunk / 8 points and walks it 32 at a
+// time; per class (left / right / pivot-bin candidate) a ballot ranks the
+// lanes, so every store instruction writes one contiguous run per class
+// (the order inside a child's segment is irrelevant to the algorithm).
 template <int SC, int D>
 __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs a)
 {
-  constexpr int PER = kChunk / kGThreads;
-  static_assert(PER <= 16, "2-bit class codes packed in one uint32");
-  __shared__ uint32_t warpTot[kGThreads / 32][3];
-  __shared__ uint32_t base[3];
+  constexpr int W = kGThreads / 32;
+  constexpr int PER_WARP = kChunk / W;
+  constexpr int ROUNDS = PER_WARP / 32;
+  static_assert(ROUNDS <= 16, "2-bit class codes packed in one uint32");
+  __shared__ uint32_t warpTot[W][3];
+  __shared__ uint32_t warpBase[W][3];
   const int seg = blockIdx.x / a.chunksPerSeg;
   const int chunk = blockIdx.x % a.chunksPerSeg;
   const SegGeo sg = seg_geo(a, seg);
@@ -376,47 +382,41 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
   const uint32_t pb = b.sel[seg * 3 + 0];
   const int cb = a.cb, nbuf = cb ^ 1;
   const uint32_t *__restrict__ kd = b.key[cb][dim] + sb;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t ltMask = (1u << lane) - 1u;
+  const int64_t w0 = c0 + int64_t(wid) * PER_WARP;
 
-  // pass 1: class 0 = left, 1 = right, 2 = candidate
+  // pass 1: class 0 = left, 1 = right, 2 = candidate; per-warp counts
   uint32_t cls = 0;
   uint32_t cnt[3] = {0, 0, 0};
 #pragma unroll
-  for (int j = 0; j < PER; j++) {
-    const int64_t i = c0 + threadIdx.x + int64_t(j) * kGThreads;
+  for (int r = 0; r < ROUNDS; r++) {
+    const int64_t i = w0 + r * 32 + lane;
+    uint32_t c = 3;
     if (i < c1) {
       const uint32_t bb = uint32_t(bin(kd[i]));
-      const uint32_t c = bb < pb ? 0u : (bb > pb ? 1u : 2u);
-      cls |= c << (2 * j);
-      cnt[c]++;
+      c = bb < pb ? 0u : (bb > pb ? 1u : 2u);
     }
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint32_t excl[3];
+    cls |= (c & 3u) << (2 * r);
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    uint32_t v = cnt[c];
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += t;
-    }
-    excl[c] = v - cnt[c];
-    if (lane == 31) warpTot[wid][c] = v;
+    for (int x = 0; x < 3; x++) cnt[x] += __popc(__ballot_sync(0xffffffffu, c == uint32_t(x)));
   }
+  if (lane < 3) warpTot[wid][lane] = cnt[lane];
   __syncthreads();
   if (threadIdx.x < 3) {
     const int c = threadIdx.x;
     uint32_t tot = 0;
-    for (int w = 0; w < kGThreads / 32; w++) {
-      uint32_t t = warpTot[w][c];
-      warpTot[w][c] = tot;
-      tot += t;
+    for (int w = 0; w < W; w++) {
+      warpBase[w][c] = tot;
+      tot += warpTot[w][c];
     }
-    base[c] = tot ? atomicAdd(&b.cur[seg * 3 + c], tot) : 0u;
+    const uint32_t base = tot ? atomicAdd(&b.cur[seg * 3 + c], tot) : 0u;
+    for (int w = 0; w < W; w++) warpBase[w][c] += base;
   }
   __syncthreads();
   uint32_t pos[3];
 #pragma unroll
-  for (int c = 0; c < 3; c++) pos[c] = base[c] + warpTot[wid][c] + excl[c];
+  for (int c = 0; c < 3; c++) pos[c] = warpBase[wid][c];
 
   const int64_t lchild = 2 * g + 1;
   const int lvlNext = a.level + 1;
@@ -430,22 +430,28 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
       lo[s][d] = 0xffffffffu;
       hi[s][d] = 0u;
     }
-#pragma unroll
-  for (int j = 0; j < PER; j++) {
-    const int64_t i = c0 + threadIdx.x + int64_t(j) * kGThreads;
-    if (i < c1) {
-      const uint32_t c = (cls >> (2 * j)) & 3u;
+  // pass 2: coalesced reads, one contiguous write run per class per round
+#pragma unroll 4
+  for (int r = 0; r < ROUNDS; r++) {
+    const int64_t i = w0 + r * 32 + lane;
+    const uint32_t c = (cls >> (2 * r)) & 3u;
+    const uint32_t m0 = __ballot_sync(0xffffffffu, c == 0u);
+    const uint32_t m1 = __ballot_sync(0xffffffffu, c == 1u);
+    const uint32_t m2 = __ballot_sync(0xffffffffu, c == 2u);
+    if (c < 3u) {
+      const uint32_t mc = c == 0u ? m0 : (c == 1u ? m1 : m2);
+      const uint32_t rank = pos[c] + __popc(mc & ltMask);
       uint32_t k[D];
 #pragma unroll
       for (int d = 0; d < D; d++) k[d] = b.key[cb][d][sb + i];
       const uint32_t id = b.idx[cb][sb + i];
-      if (c == 2) {
-        const int64_t dst = sb + pos[2]++;
+      if (c == 2u) {
+        const int64_t dst = sb + rank;
 #pragma unroll
         for (int d = 0; d < D; d++) b.ckey[d][dst] = k[d];
         b.cidx[dst] = id;
       } else {
-        const int64_t dst = (c == 0 ? lBeg : rBeg) + pos[c]++;
+        const int64_t dst = (c == 0u ? lBeg : rBeg) + rank;
 #pragma unroll
         for (int d = 0; d < D; d++) {
           b.key[nbuf][d][dst] = k[d];
@@ -455,6 +461,9 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
         b.idx[nbuf][dst] = id;
       }
     }
+    pos[0] += __popc(m0);
+    pos[1] += __popc(m1);
+    pos[2] += __popc(m2);
   }
   merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
 }
@@ -652,13 +661,14 @@ struct SubSmem {
   uint32_t idx[TILE];
   uint16_t list[2][D][TILE];
   uint16_t segOf[2][TILE];
-  uint32_t scan[TILE];
   union {
-    unsigned long long sortbuf[TILE];
-    struct {
-      uint16_t t0[TILE], t1[TILE], b[TILE], r[TILE];
-    } sub;
-  } u;
+    uint32_t scan[TILE];                 // level partitions
+    uint16_t rh[kSubThreads / 32][256];  // presort: per-warp digit counts / offsets
+  };
+  struct {
+    uint16_t t0[TILE], t1[TILE], b[TILE], r[TILE];
+  } u_sub;
+  uint32_t red[2 * (kSubThreads / 32)];
   uint16_t locPivot[2 * TILE];
   uint8_t locDim[2 * TILE];
   uint8_t flag[TILE];
@@ -668,6 +678,107 @@ struct SubSmem {
   uint32_t qcount;
   uint32_t rootLo[D], rootHi[D];
 };
+
+// Stable LSD radix sort (8-bit digits) of the indices 0..m-1 by key[i]:
+// keys are sorted over their span (key - min), so 0 to 4 passes.  Warp w
+// owns a contiguous run of positions; match_any ranks equal digits inside a
+// round of 32, per-warp digit counts scanned digit-major order the warps.
+// Result in `a`; `tmp` is scratch of m entries.
+__device__ void sub_radix_sort(const uint32_t *__restrict__ key, int m, uint16_t *a,
+                               uint16_t *tmp, uint16_t (*rh)[256], uint32_t *red)
+{
+  constexpr int W = kSubThreads / 32;
+  static_assert(kSubThreads == 256, "one thread per digit in the scan");
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  uint32_t lo = 0xffffffffu, hi = 0u;
+  for (int i = tid; i < m; i += kSubThreads) {
+    const uint32_t k = key[i];
+    lo = min(lo, k);
+    hi = max(hi, k);
+    a[i] = uint16_t(i);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if (lane == 0) {
+    red[wid] = lo;
+    red[W + wid] = hi;
+  }
+  __syncthreads();
+  uint32_t kmin = 0xffffffffu, kmax = 0u;
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    kmin = min(kmin, red[w]);
+    kmax = max(kmax, red[W + w]);
+  }
+  __syncthreads();
+  const uint32_t span = kmax >= kmin ? kmax - kmin : 0u;
+  const int bits = span ? 32 - __clz(span) : 0;
+  const int passes = (bits + 7) >> 3;
+  const int per = (m + W - 1) / W;
+  const int w0 = min(m, wid * per), w1 = min(m, w0 + per);
+  const uint32_t ltMask = (1u << lane) - 1u;
+  uint16_t *src = a, *dst = tmp;
+  for (int ps = 0; ps < passes; ps++) {
+    const int shift = ps * 8;
+    for (int i = tid; i < W * 256; i += kSubThreads) (&rh[0][0])[i] = 0;
+    __syncthreads();
+    for (int base = w0; base < w1; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < w1;
+      const uint32_t dg = valid ? ((key[src[i]] - kmin) >> shift) & 255u : 256u + lane;
+      const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+      if (valid && (peers & ltMask) == 0) rh[wid][dg] += uint16_t(__popc(peers));
+    }
+    __syncthreads();
+    {
+      // digit-major exclusive offsets: thread = digit
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < W; w++) {
+        const uint32_t c = rh[w][tid];
+        rh[w][tid] = uint16_t(run);
+        run += c;
+      }
+      uint32_t incl = run;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) red[wid] = incl;
+      __syncthreads();
+      uint32_t wbase = 0;
+      for (int w = 0; w < wid; w++) wbase += red[w];
+      const uint32_t dbase = wbase + incl - run;
+#pragma unroll
+      for (int w = 0; w < W; w++) rh[w][tid] = uint16_t(rh[w][tid] + dbase);
+    }
+    __syncthreads();
+    for (int base = w0; base < w1; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < w1;
+      const uint16_t v = valid ? src[i] : uint16_t(0);
+      const uint32_t dg = valid ? ((key[v] - kmin) >> shift) & 255u : 256u + lane;
+      const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+      const uint32_t pos = valid ? uint32_t(rh[wid][dg]) + __popc(peers & ltMask) : 0u;
+      __syncwarp();
+      if (valid) {
+        dst[pos] = v;
+        if ((peers & ltMask) == 0) rh[wid][dg] = uint16_t(rh[wid][dg] + __popc(peers));
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    uint16_t *t = src;
+    src = dst;
+    dst = t;
+  }
+  if (src != a) {
+    for (int i = tid; i < m; i += kSubThreads) a[i] = src[i];
+    __syncthreads();
+  }
+}
 
 // Finishes the subtree under node s (level L0) of a tree of n records whose
 // first record sits at `base` of the working arrays; `boxIndex` selects the
@@ -693,34 +804,9 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
   }
   __syncthreads();
 
-  // one coordinate-sorted index list per dimension (bitonic sort of
-  // key << 32 | index; equal keys in any order)
-  int P = 1;
-  while (P < m) P <<= 1;
-  for (int d = 0; d < D; d++) {
-    for (int i = tid; i < P; i += kSubThreads)
-      S.u.sortbuf[i] = i < m ? ((unsigned long long)S.key[d][i] << 32) | uint32_t(i)
-                             : ~0ull;
-    __syncthreads();
-    for (int k = 2; k <= P; k <<= 1) {
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int i = tid; i < P; i += kSubThreads) {
-          const int l = i ^ j;
-          if (l > i) {
-            const unsigned long long x = S.u.sortbuf[i], y = S.u.sortbuf[l];
-            const bool up = (i & k) == 0;
-            if ((x > y) == up) {
-              S.u.sortbuf[i] = y;
-              S.u.sortbuf[l] = x;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    }
-    for (int i = tid; i < m; i += kSubThreads) S.list[0][d][i] = uint16_t(S.u.sortbuf[i]);
-    __syncthreads();
-  }
+  // one coordinate-sorted index list per dimension (equal keys in any
+  // order; runs of equal keys are ranked by the composite key below)
+  for (int d = 0; d < D; d++) sub_radix_sort(S.key[d], m, S.list[0][d], S.list[1][d], S.rh, S.red);
 
   int cur = 0;
   int mact = m;
@@ -786,10 +872,10 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
           hi = mid;
       }
       const int t1 = lo;
-      S.u.sub.t0[t] = uint16_t(t0);
-      S.u.sub.t1[t] = uint16_t(t1);
-      S.u.sub.b[t] = uint16_t(bt);
-      S.u.sub.r[t] = uint16_t(r);
+      S.u_sub.t0[t] = uint16_t(t0);
+      S.u_sub.t1[t] = uint16_t(t1);
+      S.u_sub.b[t] = uint16_t(bt);
+      S.u_sub.r[t] = uint16_t(r);
       S.subDim[t] = uint8_t(dim);
       if (t1 - t0 == 1) {
         const int piv = Ld[pp];
@@ -808,8 +894,8 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
       const int64_t g = g0 + t;
       const int u = (1 << j) - 1 + t;
       const int dim = S.subDim[t];
-      const int t0 = S.u.sub.t0[t], t1 = S.u.sub.t1[t];
-      const int pp = S.u.sub.b[t] + S.u.sub.r[t];
+      const int t0 = S.u_sub.t0[t], t1 = S.u_sub.t1[t];
+      const int pp = S.u_sub.b[t] + S.u_sub.r[t];
       int cd[D];
       int ncd = 0;
       cd[ncd++] = dim;
@@ -866,9 +952,9 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     for (int p = tid; p < mact; p += kSubThreads) {
       const int t = S.segOf[cur][p];
       const int e = S.list[cur][S.subDim[t]][p];
-      if (p < S.u.sub.t0[t])
+      if (p < S.u_sub.t0[t])
         S.flag[e] = 0;
-      else if (p >= S.u.sub.t1[t])
+      else if (p >= S.u_sub.t1[t])
         S.flag[e] = 1;
     }
     __syncthreads();
@@ -911,11 +997,11 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
         const int f = S.flag[e];
         if (f == 2) continue;
         const int t = S.segOf[cur][p];
-        const int bt = S.u.sub.b[t];
+        const int bt = S.u_sub.b[t];
         const uint32_t sbase = S.scan[bt], sp = S.scan[p];
         const int nb = bt - t;
         const int np = f == 0 ? nb + int((sp & 0xffffu) - (sbase & 0xffffu))
-                              : nb + S.u.sub.r[t] + int((sp >> 16) - (sbase >> 16));
+                              : nb + S.u_sub.r[t] + int((sp >> 16) - (sbase >> 16));
         S.list[cur ^ 1][d][np] = uint16_t(e);
         if (d == 0) S.segOf[cur ^ 1][np] = uint16_t(2 * t + f);
       }

@@ -29,52 +29,76 @@ __global__ void __launch_bounds__(kThreads) upsweep_kernel(const uint32_t *__res
   counts[int64_t(threadIdx.x) * numTiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// single-CTA exclusive scan of `len` counts
-__global__ void __launch_bounds__(1024) scan_kernel(uint32_t *counts, int64_t len)
+// exclusive scan of one digit's column of per-tile counts (one CTA per
+// digit, counts stored digit-major); the column total goes to digitTotals
+__global__ void __launch_bounds__(kThreads) column_scan_kernel(uint32_t *counts, int numTiles,
+                                                               uint32_t *digitTotals)
 {
-  __shared__ uint32_t warpSums[32];
+  __shared__ uint32_t warpSums[kThreads / 32];
   __shared__ uint32_t carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t *col = counts + int64_t(blockIdx.x) * numTiles;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t off = 0; off < len; off += 1024) {
-    const int64_t i = off + threadIdx.x;
-    const uint32_t v = i < len ? counts[i] : 0u;
-    uint32_t incl = v;
+  constexpr int PER = 4;
+  for (int off = 0; off < numTiles; off += kThreads * PER) {
+    uint32_t v[PER], s = 0;
+    const int b = off + threadIdx.x * PER;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      v[j] = b + j < numTiles ? col[b + j] : 0u;
+      s += v[j];
+    }
+    uint32_t incl = s;
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += t;
     }
     if (lane == 31) warpSums[wid] = incl;
     __syncthreads();
-    if (wid == 0) {
-      const uint32_t s = warpSums[lane];
-      uint32_t si = s;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, si, o);
-        if (lane >= o) si += t;
-      }
-      warpSums[lane] = si - s;
+    uint32_t wbase = 0, tot = 0;
+    for (int w = 0; w < kThreads / 32; w++) {
+      const uint32_t x = warpSums[w];
+      wbase += w < wid ? x : 0u;
+      tot += x;
+    }
+    uint32_t run = carry + wbase + incl - s;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      if (b + j < numTiles) col[b + j] = run;
+      run += v[j];
     }
     __syncthreads();
-    const uint32_t c = carry;
-    if (i < len) counts[i] = c + warpSums[wid] + incl - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) carry = c + warpSums[wid] + incl;
+    if (threadIdx.x == 0) carry += tot;
     __syncthreads();
   }
+  if (threadIdx.x == 0) digitTotals[blockIdx.x] = carry;
 }
 
 __global__ void __launch_bounds__(kThreads) scatter_kernel(
     const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, int64_t n, int shift,
-    int numTiles, const uint32_t *__restrict__ offsets, uint32_t *__restrict__ keysOut,
-    uint32_t *__restrict__ valsOut)
+    int numTiles, const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ digitTotals,
+    uint32_t *__restrict__ keysOut, uint32_t *__restrict__ valsOut)
 {
   constexpr int W = kThreads / 32;
   __shared__ uint32_t running[256];
   __shared__ uint32_t wcnt[W][256];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  running[threadIdx.x] = offsets[int64_t(threadIdx.x) * numTiles + blockIdx.x];
+  {
+    // exclusive prefix of the 256 digit totals (computed by every CTA)
+    const uint32_t t = digitTotals[threadIdx.x];
+    uint32_t incl = t;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) wcnt[0][wid] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < wid; w++) wbase += wcnt[0][w];
+    running[threadIdx.x] = offsets[int64_t(threadIdx.x) * numTiles + blockIdx.x] + wbase + incl - t;
+    __syncthreads();
+  }
   for (int w = 0; w < W; w++) wcnt[w][threadIdx.x] = 0;
   __syncthreads();
   const int64_t base = int64_t(blockIdx.x) * kTileItems;
@@ -111,7 +135,7 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(
 
 }  // namespace
 
-int64_t radix_sort_counts(int64_t n) { return std::max<int64_t>(1, div_up(n, kTileItems)) * 256; }
+int64_t radix_sort_counts(int64_t n) { return (std::max<int64_t>(1, div_up(n, kTileItems)) + 1) * 256; }
 
 int radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys2, uint32_t *vals2,
                      int64_t n, int bits, cudaStream_t st, TempArena *arena)
@@ -127,14 +151,16 @@ int radix_sort_pairs_ws(uint32_t *keys, uint32_t *vals, uint32_t *keys2, uint32_
 {
   if (n <= 1 || bits <= 0) return CUKD_OK;
   const int numTiles = int(div_up(n, kTileItems));
+  uint32_t *totals = counts + int64_t(numTiles) * 256;  // 256 digit totals
   uint32_t *ka = keys, *va = vals, *kb = keys2, *vb = vals2;
   int passes = 0;
   for (int shift = 0; shift < bits; shift += 8, passes++) {
     upsweep_kernel<<<numTiles, kThreads, 0, st>>>(ka, n, shift, numTiles, counts);
     CKB_CHECK_LAUNCH();
-    scan_kernel<<<1, 1024, 0, st>>>(counts, int64_t(numTiles) * 256);
+    column_scan_kernel<<<256, kThreads, 0, st>>>(counts, numTiles, totals);
     CKB_CHECK_LAUNCH();
-    scatter_kernel<<<numTiles, kThreads, 0, st>>>(ka, va, n, shift, numTiles, counts, kb, vb);
+    scatter_kernel<<<numTiles, kThreads, 0, st>>>(ka, va, n, shift, numTiles, counts, totals, kb,
+                                                  vb);
     CKB_CHECK_LAUNCH();
     std::swap(ka, kb);
     std::swap(va, vb);

@@ -245,3 +245,19 @@ def test_config3_shape_sampled_parity():
         i, d, _ = po.knn(t, q, 8, po.STACK_BASED, bounds=b0)
         assert np.array_equal(ids[qoff[c]:qoff[c + 1]], i), c
         assert np.array_equal(f32_bits(d2[qoff[c]:qoff[c + 1]]), f32_bits(d)), c
+
+
+def test_large_query_cloud_takes_global_morton_sort():
+    """A cloud with more queries than the per-cloud shared-memory sort holds
+    sends the whole batch through the global radix sort: same answers."""
+    rng = np.random.Generator(np.random.MT19937(71))
+    sizes = np.array([5000, 300, 0, 2500], np.int64)
+    nqs = np.array([9000, 50, 10, 0], np.int64)
+    pts = rng.random((int(sizes.sum()), 3)).astype(np.float32)
+    qs = rng.random((int(nqs.sum()), 3)).astype(np.float32)
+    poff = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    qoff = np.concatenate([[0], np.cumsum(nqs)]).astype(np.int64)
+    ref = _oracle(pts, poff, qs, qoff, 8, po.STACK_BASED)
+    plan = ck.BatchPlan(poff, qoff, 3, k=8)
+    built, bnd, got = _run_build_query(plan, pts, qs)
+    _check(plan, pts, poff, qs, qoff, ref, bnd, built, got)
