@@ -148,6 +148,21 @@ def profile_traffic(key):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def max_over_ranks(t_ms, pg, device):
+    """The slowest rank's device time (every rank takes the same collective)."""
+    if not pg:
+        return float(t_ms)
+    import torch
+    t = torch.tensor([float(t_ms)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms_per_step):
+    """Units all ranks processed per second (weak scaling: fixed work per rank)."""
+    return world * units_per_rank / (ms_per_step / 1e3)
+
+
 def run_ours(args, rank, world, local):
     import torch
     import cudakdtree_b200 as ck
@@ -201,13 +216,9 @@ def run_ours(args, rank, world, local):
     barrier()
     launches = ck.launch_count() - l0
     clocks = sampler.stop()
-    t_ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([t_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_ms = float(t.item())
+    t_ms = max_over_ranks(e0.elapsed_time(e1), pg, dev)
     ms_per_step = t_ms / args.steps
-    value = world * nq / (ms_per_step / 1e3)
+    value = whole_job_rate(nq, world, ms_per_step)
 
     # ---- phase timings (same stream, CUDA events), outside the timed region
     def timed(fn, reps=3):
@@ -313,12 +324,8 @@ def run_ours(args, rank, world, local):
             e2e_step()
         b.record()
         barrier()
-        et = a.elapsed_time(b)
-        if pg:
-            t = torch.tensor([et], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            et = float(t.item())
-        e2e = {"value": round(world * nq / (et / args.steps / 1e3), 1), "unit": UNIT,
+        et = max_over_ranks(a.elapsed_time(b), pg, dev)
+        e2e = {"value": round(whole_job_rate(nq, world, et / args.steps), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(h_pts.numel() * 4 + h_q.numel() * 4),
                "d2h_bytes_per_step": int(h_ids.numel() * 4 + h_d2.numel() * 4),
                "ms_per_step": round(et / args.steps, 3)}
