@@ -33,7 +33,8 @@ __all__ = [
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libcukd_b200.so")
+# the in-tree build; CUKD_B200_LIBRARY names another build of the same library
+LIB_PATH = os.environ.get("CUKD_B200_LIBRARY") or os.path.join(HERE, "lib", "libcukd_b200.so")
 
 FLOAT32, INT32 = 0, 1
 STACK_BASED, STACK_FREE, CCT = 0, 1, 2
