@@ -418,8 +418,8 @@ static int query_impl(cukd_batch_plan_s *p, const float *pts, const float *bound
     a.order = (const int32_t *)p->mvals;
   }
   const bool fastOk = !p->fcp && !a.heap_order && !(p->params.flags & CUKD_QUERY_REFERENCE_ORDER) &&
-                      !(p->params.flags & CUKD_QUERY_FORCE_HEAP) && p->params.k >= 2 &&
-                      p->params.k <= 32;
+                      p->params.k >= 2 &&
+                      p->params.k <= 128;
   if (fastOk) {
     fast::FastArgs fa = {};
     fa.q = a;

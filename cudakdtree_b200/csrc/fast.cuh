@@ -20,7 +20,8 @@ struct FastArgs {
 
 }  // namespace fast
 
-// Launches the fast kernel for float trees with D = 2..4 and k + 1 <= 33.
+// Launches the fast kernel for float trees with D = 2..4 and k <= 128
+// (register list up to k = 32, local-memory heap above).
 int run_fast(const fast::FastArgs &fa, int D, cudaStream_t st);
 
 }  // namespace ckb

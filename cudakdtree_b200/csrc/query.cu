@@ -178,7 +178,7 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   // reference-order re-run of the queued queries
   const bool fastOk = L.scalar == CUKD_FLOAT32 && !visits && !a.heap_order &&
                       !(p->flags & CUKD_QUERY_REFERENCE_ORDER) &&
-                      knn && p->k >= 2 && p->k <= 32 && n < (int64_t(1) << 31) - 1;
+                      knn && p->k >= 2 && p->k <= 128 && n < (int64_t(1) << 31) - 1;
   // (FCP and k = 1 stay on the reference traversals: with a single
   // candidate the split-plane bound is already cheap and the corner
   // bookkeeping does not pay for itself)

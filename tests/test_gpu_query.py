@@ -69,7 +69,7 @@ def test_fcp(mname, m, kind, explicit, cutoff, morton):
 
 
 @pytest.mark.parametrize("mname,m", METHODS)
-@pytest.mark.parametrize("k", [1, 4, 5, 8, 16, 20, 32, 50, 64])
+@pytest.mark.parametrize("k", [1, 4, 5, 8, 16, 20, 32, 33, 50, 64, 65, 128, 129, 200])
 @pytest.mark.parametrize("kind", ["uniform", "tie"])
 def test_knn(mname, m, k, kind):
     n, nq = 20000, 8000
@@ -104,8 +104,9 @@ def test_knn_heap_order(mname, m, k):
 @pytest.mark.parametrize("explicit", [False, True])
 @pytest.mark.parametrize("D", [2, 4])
 @pytest.mark.parametrize("cutoff", [math.inf, 0.1])
-def test_knn_dims_cutoff(mname, m, explicit, D, cutoff):
-    n, nq, k = 10000, 5000, 8
+@pytest.mark.parametrize("k", [8, 64])
+def test_knn_dims_cutoff(mname, m, explicit, D, cutoff, k):
+    n, nq = 10000, 5000
     tree, dims, bounds = _tree(n, D, "uniform", explicit, seed=D)
     q = make_queries(nq, D, "uniform", seed=D + 1)
     ri, rd, _ = po.knn(tree, q, k, m, dims=dims, bounds=bounds, cutoff=cutoff)
