@@ -37,8 +37,6 @@ K = 16
 RECORD_BYTES = 16
 METRIC = "knn_queries_per_s"
 UNIT = "queries/s"
-WORKLOAD = ("build (widest-dim, 16-byte {float3,payload+dim} records) + kNN k=16 "
-            "stack-based over 10M Gaussian-mixture points and 10M mixture queries")
 
 
 def parse():
@@ -53,6 +51,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--configs", default="",
+                    help="comma list of c1,c2,c4,c5: measure those configurations instead "
+                         "(one JSON line each, not the benchmark line)")
     return ap.parse_args()
 
 
@@ -61,6 +62,13 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def workload_desc(n, nq):
+    def m(x):
+        return f"{x / 1e6:g}M" if x >= 1e6 else str(x)
+    return (f"build (widest-dim, 16-byte {{float3,payload+dim}} records) + kNN k={K} "
+            f"stack-based over {m(n)} Gaussian-mixture points and {m(nq)} mixture queries")
 
 
 def workload(n_points, n_queries):
@@ -340,7 +348,7 @@ def run_ours(args, rank, world, local):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded Gaussian mixture, 64 components, sigma 0.01)",
-           "config": {"workload": WORKLOAD, "points": n, "queries": nq, "k": K,
+           "config": {"workload": workload_desc(n, nq), "points": n, "queries": nq, "k": K,
                       "record_bytes": RECORD_BYTES, "split": "widest extent (explicit dim)",
                       "traversal": "stack_based", "morton_reorder": True,
                       "l2": "inputs exceed L2 (160 MB points + 120 MB queries), no flush",
@@ -482,23 +490,312 @@ def run_reference(args, rank, world, local):
             f"{n} points timed once ({t_build:.2f} s) + stackBased::knn<FixedCandidateList<16>> "
             f"on {sample}-query samples per step with {cores} OpenMP threads, scaled to {nq} "
             "queries")
+    ref_gpu = reference_gpu_timings(recs, q)
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (same seeds as our arm)",
-           "config": {"workload": WORKLOAD, "points": n, "queries": nq, "k": K,
+           "config": {"workload": workload_desc(n, nq), "points": n, "queries": nq, "k": K,
                       "parallelism": "host cores"},
            "build_ms": round(t_build * 1e3, 1),
            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores,
                             "kind": "reference", "sample": desc},
            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
-                   "d2h_bytes_per_step": 0}}
+                   "d2h_bytes_per_step": 0},
+           "reference_gpu": ref_gpu}
     print(json.dumps(out), flush=True)
+
+
+def reference_gpu_timings(recs, q):
+    """For context beside the CPU arm: the reference's own GPU builders and
+    traversal (compiled unmodified from its headers into oracle/_ref) on the
+    same records and queries, on this GPU, timed with CUDA events.  Not part
+    of the arm's value."""
+    try:
+        import ctypes as C
+        import torch
+        from oracle import pyoracle as po
+        if not torch.cuda.is_available() or po.ref_gpu() is None:
+            return {"unavailable": "no GPU or oracle/_ref GPU library not built"}
+        L = po.ref_gpu()
+        n, nq = len(recs), len(q)
+        src = torch.from_numpy(recs.view(np.uint8).copy()).cuda()
+        d = torch.empty_like(src)
+        wb = torch.zeros((2, 3), dtype=torch.float32, device="cuda")
+        dq = torch.from_numpy(q).cuda()
+        ids = torch.empty((nq, K), dtype=torch.int32, device="cuda")
+        d2 = torch.empty((nq, K), dtype=torch.float32, device="cuda")
+
+        def timed(fn):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            rc = fn()
+            b.record()
+            torch.cuda.synchronize()
+            if rc != 0:
+                raise RuntimeError(f"reference GPU call failed: {rc}")
+            return a.elapsed_time(b)
+
+        res = {}
+        for builder, name in ((0, "buildTree_thrust"), (1, "buildTree_bitonic")):
+            ts = []
+            for _ in range(2):
+                d.copy_(src)
+                ts.append(timed(lambda: L.refg_build(po.REF_F3_PACKED, builder,
+                                                     C.c_void_p(d.data_ptr()), n,
+                                                     C.c_void_p(wb.data_ptr()))))
+            res[name + "_ms"] = round(min(ts), 3)
+        hb = np.ascontiguousarray(wb.cpu().numpy())
+        knn = lambda: L.refg_knn(po.REF_F3_PACKED, 0, 0, K, C.c_void_p(d.data_ptr()), n,
+                                 hb.ctypes.data_as(C.c_void_p), C.c_void_p(dq.data_ptr()), nq,
+                                 float("inf"), C.c_void_p(ids.data_ptr()),
+                                 C.c_void_p(d2.data_ptr()))
+        timed(knn)
+        t_knn = min(timed(knn) for _ in range(2))
+        res["stackBased_knn_k16_ms"] = round(t_knn, 3)
+        res["knn_queries_per_s"] = round(nq / (t_knn / 1e3), 1)
+        res["build_plus_knn_queries_per_s"] = round(
+            nq / ((res["buildTree_thrust_ms"] + t_knn) / 1e3), 1)
+        res["note"] = ("reference code compiled unmodified with -fmad=false, one thread per "
+                       "query in input order (testing/floatN-knn-and-fcp.cu pattern)")
+        return res
+    except Exception as e:  # context only: never fail the arm
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
+# ---------------------------------------------------------------------------
+# the other configurations (parity-test workloads), measured on request
+# ---------------------------------------------------------------------------
+def _timer():
+    import torch
+
+    def timed(fn, reps=3, setup=None):
+        if setup:
+            setup()
+        fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            if setup:
+                setup()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+    return timed
+
+
+def config_c1(ck, dev):
+    """1M U[0,1)^3 float3 points (seed 1), 1M U[0,1)^3 queries (seed 2),
+    round-robin dims; FCP and kNN k=8 with the three traversals; the
+    reference's host build + host traversals on the same data for context."""
+    import torch
+    from cudakdtree_b200 import workloads as wl
+    timed = _timer()
+    pts = wl.uniform_points(1_000_000, seed=1)
+    q = wl.uniform_points(1_000_000, seed=2)
+    src = torch.from_numpy(pts).to(dev)
+    P = torch.empty_like(src)
+    Q = torch.from_numpy(q).to(dev)
+    lay = ck.layout_for("float32", 3)
+    wb = torch.empty((2, 3), dtype=torch.float32, device=dev)
+    copy = lambda: P.copy_(src)
+    build_ms = timed(lambda: ck.build_tree(P, layout=lay, world_bounds=wb), reps=5, setup=copy)
+    out = {"config": "C1", "workload": "1M uniform float3, 1M uniform queries, round-robin",
+           "build_ms": round(build_ms, 3), "queries_per_s": {}}
+    for m in ("stack_based", "stack_free", "cct"):
+        t = timed(lambda: ck.fcp(P, Q, m, layout=lay, world_bounds=wb))
+        out["queries_per_s"][f"fcp_{m}"] = round(len(q) / (t / 1e3), 1)
+        t = timed(lambda: ck.knn(P, Q, 8, m, layout=lay, world_bounds=wb))
+        out["queries_per_s"][f"knn8_{m}"] = round(len(q) / (t / 1e3), 1)
+    try:
+        from oracle import pyoracle as po
+        if po.ref_host() is not None:
+            t0 = time.perf_counter()
+            tree, bounds = po.ref_build_host(po.REF_F3, pts)
+            tb = time.perf_counter() - t0
+            qs = np.ascontiguousarray(q[:200_000])
+            t0 = time.perf_counter()
+            po.ref_fcp_host(po.REF_F3, tree, bounds, qs, po.CCT)
+            tf = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            po.ref_knn_host(po.REF_F3, tree, bounds, qs, 8, po.STACK_BASED)
+            tk = time.perf_counter() - t0
+            out["cpu_reference"] = {"cores": po.nthreads(), "buildTree_host_ms": round(tb * 1e3, 1),
+                                    "cct_fcp_queries_per_s": round(len(qs) / tf, 1),
+                                    "stackBased_knn8_queries_per_s": round(len(qs) / tk, 1),
+                                    "sample": "200K of the 1M queries"}
+    except Exception as e:
+        out["cpu_reference"] = {"unavailable": str(e)}
+    return out
+
+
+def config_c2(ck, dev):
+    """The benchmark workload's data with every builder name, the spatial
+    tree, and kNN k=16 with the three traversals."""
+    import torch
+    timed = _timer()
+    recs, q = workload(N_POINTS, N_QUERIES)
+    n, nq = len(recs), len(q)
+    lay = ck.layout_for("float32", 3, stride=RECORD_BYTES, dim_offset=12, dim_shift=30,
+                        dim_bits=2)
+    src = torch.from_numpy(recs.view(np.int32).reshape(n, 4).copy()).to(dev)
+    P = torch.empty_like(src)
+    Q = torch.from_numpy(q).to(dev)
+    wb = torch.empty((2, 3), dtype=torch.float32, device=dev)
+    copy = lambda: P.copy_(src)
+    out = {"config": "C2", "workload": workload_desc(n, nq), "build_ms": {}, "queries_per_s": {}}
+    for b in ("thrust", "bitonic", "inplace"):
+        out["build_ms"][b] = round(timed(lambda: ck.build_tree(P, layout=lay, world_bounds=wb,
+                                                               builder=b), setup=copy), 3)
+    lay_pts = ck.layout_for("float32", 3, stride=RECORD_BYTES)
+    sp = [None]
+
+    def spatial():
+        if sp[0] is not None:
+            sp[0].free()
+        sp[0] = ck.spatial_build(src, layout=lay_pts)
+    out["build_ms"]["spatial"] = round(timed(spatial), 3)
+    t = timed(lambda: sp[0].knn(Q, K, "cct"))
+    out["queries_per_s"]["spatial_knn16_cct"] = round(nq / (t / 1e3), 1)
+    sp[0].free()
+    copy()
+    ck.build_tree(P, layout=lay, world_bounds=wb)
+    for m in ("stack_based", "stack_free", "cct"):
+        t = timed(lambda: ck.knn(P, Q, K, m, layout=lay, world_bounds=wb))
+        out["queries_per_s"][f"knn16_{m}"] = round(nq / (t / 1e3), 1)
+    t = timed(lambda: ck.fcp(P, Q, "stack_based", layout=lay, world_bounds=wb))
+    out["queries_per_s"]["fcp_stack_based"] = round(nq / (t / 1e3), 1)
+    return out
+
+
+def config_c4(ck, dev):
+    """Learned radius at k = 32: model trained on 1M mixture queries, then
+    50M queries (70% mixture / 30% uniform) answered plain and learned."""
+    import torch
+    from cudakdtree_b200 import workloads as wl
+    timed = _timer()
+    recs, _ = workload(N_POINTS, 1)
+    n = len(recs)
+    lay = ck.layout_for("float32", 3, stride=RECORD_BYTES, dim_offset=12, dim_shift=30,
+                        dim_bits=2)
+    P = torch.from_numpy(recs.view(np.int32).reshape(n, 4).copy()).to(dev)
+    wb = ck.build_tree(P, layout=lay)
+    k = 32
+    qtrain = torch.from_numpy(wl.gmm_points(1_000_000, seed=3, sample_seed=14)).to(dev)
+    model = ck.RadiusModel(grid_res=64, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    model.fit(P, qtrain, k, layout=lay, world_bounds=wb, epochs=10, batch=4096)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    nq = 50_000_000
+    Q = torch.from_numpy(wl.mixed_queries(nq)).to(dev)
+    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    d2 = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    t_plain = timed(lambda: ck.knn(P, Q, k, "stack_based", layout=lay, world_bounds=wb,
+                                   out_ids=ids, out_d2=d2), reps=2)
+    ref_ids = ids.clone()
+    fb = [None]
+
+    def learned():
+        fb[0] = ck.knn_learned(P, Q, k, model, "stack_based", layout=lay, world_bounds=wb,
+                               scale=1.2, out_ids=ids, out_d2=d2)[2]
+    t_learned = timed(learned, reps=2)
+    same = bool(torch.equal(ids, ref_ids))
+    t_ref = timed(lambda: ck.knn(P, Q[:5_000_000], k, "stack_based", layout=lay,
+                                 world_bounds=wb, reference_order=True), reps=1) * 10
+    return {"config": "C4", "workload": "10M-point mixture tree, k=32, train 1M mixture "
+            "queries, infer 50M (70% mixture / 30% uniform), radius x1.2",
+            "train_s": round(train_s, 3), "final_loss": round(model.final_loss, 5),
+            "plain_fast_ms": round(t_plain, 3), "learned_ms": round(t_learned, 3),
+            "reference_order_ms_est": round(t_ref, 1),
+            "speedup_vs_plain_fast": round(t_plain / t_learned, 3),
+            "speedup_vs_reference_order": round(t_ref / t_learned, 3),
+            "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
+            "identical_results": same}
+
+
+def config_c5(ck, dev):
+    """100M float4 points (xyz U[0,1), w N(0,1)) with widest-extent dims in a
+    {float4; int dim} record, and 20M int3 points in [-2^20, 2^20]^3 with
+    round-robin dims; kNN k = 64 on 20M queries of each distribution."""
+    import torch
+    from cudakdtree_b200 import workloads as wl
+    timed = _timer()
+    out = {"config": "C5"}
+    n, nq, k = 100_000_000, 20_000_000, 64
+    p4 = wl.wide_float4(n, seed=7)
+    rec = np.zeros((n, 5), np.float32)
+    rec[:, :4] = p4
+    del p4
+    lay = ck.layout_for("float32", 4, stride=20, dim_offset=16)
+    src = torch.from_numpy(rec.view(np.uint8).reshape(-1)).to(dev)
+    del rec
+    P = torch.empty_like(src)
+    wb = torch.empty((2, 4), dtype=torch.float32, device=dev)
+    out["float4_100M_build_ms"] = round(timed(lambda: ck.build_tree(P, layout=lay, world_bounds=wb,
+                                                                    n=n),
+                                              setup=lambda: P.copy_(src), reps=2), 3)
+    del src
+    Q = torch.from_numpy(wl.wide_float4(nq, seed=9)).to(dev)
+    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    d2 = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    t = timed(lambda: ck.knn(P, Q, k, "stack_based", layout=lay, world_bounds=wb, n=n,
+                             out_ids=ids, out_d2=d2), reps=1)
+    out["float4_knn64_queries_per_s"] = round(nq / (t / 1e3), 1)
+    out["float4_learned"] = "unavailable: the learned radius model is float3-only"
+    del P, Q, ids, d2
+    torch.cuda.empty_cache()
+    pi = wl.int3_points(20_000_000, seed=8)
+    qi = wl.int3_points(nq, seed=10)
+    srci = torch.from_numpy(pi).to(dev)
+    Pi = torch.empty_like(srci)
+    layi = ck.layout_for("int32", 3)
+    wbi = torch.empty((2, 3), dtype=torch.int32, device=dev)
+    out["int3_20M_build_ms"] = round(timed(lambda: ck.build_tree(Pi, layout=layi, world_bounds=wbi),
+                                           setup=lambda: Pi.copy_(srci), reps=2), 3)
+    Qi = torch.from_numpy(qi).to(dev)
+    t = timed(lambda: ck.knn(Pi, Qi, k, "stack_based", layout=layi, world_bounds=wbi), reps=1)
+    out["int3_knn64_queries_per_s"] = round(nq / (t / 1e3), 1)
+    out["int3_learned"] = "unavailable: the learned radius model is float3-only"
+    try:
+        from oracle import pyoracle as po
+        tree = Pi.cpu().numpy()
+        qs = np.ascontiguousarray(qi[:20_000])
+        t0 = time.perf_counter()
+        po.knn(tree, qs, k, po.STACK_BASED, bounds=wbi.cpu().numpy())
+        out["int3_cpu_restatement_knn64_queries_per_s"] = round(len(qs) / (time.perf_counter() - t0), 1)
+        out["int3_cpu_note"] = (f"oracle's C restatement (the reference has no int traversal), "
+                                f"{po.nthreads()} threads, 20K-query sample")
+    except Exception as e:
+        out["int3_cpu_restatement"] = {"unavailable": str(e)}
+    return out
+
+
+def run_configs(args):
+    import torch
+    import cudakdtree_b200 as ck
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    fns = {"c1": config_c1, "c2": config_c2, "c4": config_c4, "c5": config_c5}
+    for name in [c.strip().lower() for c in args.configs.split(",") if c.strip()]:
+        res = fns[name](ck, dev)
+        print(json.dumps(res), flush=True)
+        torch.cuda.empty_cache()
 
 
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.configs:
+        if rank == 0:
+            run_configs(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world, local)
     else:
