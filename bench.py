@@ -674,8 +674,9 @@ def config_c2(ck, dev):
 
 
 def config_c4(ck, dev):
-    """Learned radius at k = 32: model trained on 1M mixture queries, then
-    50M queries (70% mixture / 30% uniform) answered plain and learned."""
+    """Learned radius at k = 32: model trained on 1M queries of the serving
+    distribution (70% mixture / 30% uniform, their own seed), then 50M such
+    queries answered plain and learned."""
     import torch
     from cudakdtree_b200 import workloads as wl
     timed = _timer()
@@ -686,7 +687,7 @@ def config_c4(ck, dev):
     P = torch.from_numpy(recs.view(np.int32).reshape(n, 4).copy()).to(dev)
     wb = ck.build_tree(P, layout=lay)
     k = 32
-    qtrain = torch.from_numpy(wl.gmm_points(1_000_000, seed=3, sample_seed=14)).to(dev)
+    qtrain = torch.from_numpy(wl.mixed_queries(1_000_000, seed=14)).to(dev)
     model = ck.RadiusModel(grid_res=64, seed=1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -709,8 +710,8 @@ def config_c4(ck, dev):
     same = bool(torch.equal(ids, ref_ids))
     t_ref = timed(lambda: ck.knn(P, Q[:5_000_000], k, "stack_based", layout=lay,
                                  world_bounds=wb, reference_order=True), reps=1) * 10
-    return {"config": "C4", "workload": "10M-point mixture tree, k=32, train 1M mixture "
-            "queries, infer 50M (70% mixture / 30% uniform), radius x1.2",
+    return {"config": "C4", "workload": "10M-point mixture tree, k=32, train on 1M and infer "
+            "50M queries (70% mixture / 30% uniform), radius x1.2",
             "train_s": round(train_s, 3), "final_loss": round(model.final_loss, 5),
             "plain_fast_ms": round(t_plain, 3), "learned_ms": round(t_learned, 3),
             "reference_order_ms_est": round(t_ref, 1),
