@@ -360,7 +360,7 @@ __device__ inline void merge_child_bounds(uint32_t (&lo)[2][D], uint32_t (&hi)[2
 // lanes, so every store instruction writes one contiguous run per class
 // (the order inside a child's segment is irrelevant to the algorithm).
 template <int SC, int D>
-__global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs a)
+__global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelArgs a)
 {
   constexpr int W = kGThreads / 32;
   constexpr int PER_WARP = kChunk / W;
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
 #pragma unroll
     for (int x = 0; x < 3; x++) cnt[x] += __popc(__ballot_sync(0xffffffffu, c == uint32_t(x)));
   }
-  if (lane < 3) warpTot[wid][lane] = cnt[lane];
+  if (lane < 3) warpTot[wid][lane] = lane == 0 ? cnt[0] : (lane == 1 ? cnt[1] : cnt[2]);
   __syncthreads();
   if (threadIdx.x < 3) {
     const int c = threadIdx.x;
@@ -430,40 +430,62 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
       lo[s][d] = 0xffffffffu;
       hi[s][d] = 0u;
     }
-  // pass 2: coalesced reads, one contiguous write run per class per round
-#pragma unroll 4
-  for (int r = 0; r < ROUNDS; r++) {
-    const int64_t i = w0 + r * 32 + lane;
-    const uint32_t c = (cls >> (2 * r)) & 3u;
-    const uint32_t m0 = __ballot_sync(0xffffffffu, c == 0u);
-    const uint32_t m1 = __ballot_sync(0xffffffffu, c == 1u);
-    const uint32_t m2 = __ballot_sync(0xffffffffu, c == 2u);
-    if (c < 3u) {
-      const uint32_t mc = c == 0u ? m0 : (c == 1u ? m1 : m2);
-      const uint32_t rank = pos[c] + __popc(mc & ltMask);
-      uint32_t k[D];
+  // pass 2: coalesced reads (four rounds' loads issued together), one
+  // contiguous write run per class per round.  Class-indexed values are
+  // picked with selects so that nothing lands in local memory.
+  constexpr int RB = 4;
+  static_assert(ROUNDS % RB == 0, "rounds in batches");
+  for (int r0 = 0; r0 < ROUNDS; r0 += RB) {
+    uint32_t kk[RB][D], idv[RB];
 #pragma unroll
-      for (int d = 0; d < D; d++) k[d] = b.key[cb][d][sb + i];
-      const uint32_t id = b.idx[cb][sb + i];
-      if (c == 2u) {
-        const int64_t dst = sb + rank;
+    for (int u = 0; u < RB; u++) {
+      const int64_t i = w0 + (r0 + u) * 32 + lane;
+      const uint32_t c = (cls >> (2 * (r0 + u))) & 3u;
+      if (c < 3u) {
 #pragma unroll
-        for (int d = 0; d < D; d++) b.ckey[d][dst] = k[d];
-        b.cidx[dst] = id;
-      } else {
-        const int64_t dst = (c == 0u ? lBeg : rBeg) + rank;
-#pragma unroll
-        for (int d = 0; d < D; d++) {
-          b.key[nbuf][d][dst] = k[d];
-          lo[c][d] = min(lo[c][d], k[d]);
-          hi[c][d] = max(hi[c][d], k[d]);
-        }
-        b.idx[nbuf][dst] = id;
+        for (int d = 0; d < D; d++) kk[u][d] = b.key[cb][d][sb + i];
+        idv[u] = b.idx[cb][sb + i];
       }
     }
-    pos[0] += __popc(m0);
-    pos[1] += __popc(m1);
-    pos[2] += __popc(m2);
+#pragma unroll
+    for (int u = 0; u < RB; u++) {
+      const uint32_t c = (cls >> (2 * (r0 + u))) & 3u;
+      const uint32_t m0 = __ballot_sync(0xffffffffu, c == 0u);
+      const uint32_t m1 = __ballot_sync(0xffffffffu, c == 1u);
+      const uint32_t m2 = __ballot_sync(0xffffffffu, c == 2u);
+      if (c < 3u) {
+        const uint32_t mc = c == 0u ? m0 : (c == 1u ? m1 : m2);
+        const uint32_t pc = c == 0u ? pos[0] : (c == 1u ? pos[1] : pos[2]);
+        const uint32_t rank = pc + __popc(mc & ltMask);
+        if (c == 2u) {
+          const int64_t dst = sb + rank;
+#pragma unroll
+          for (int d = 0; d < D; d++) b.ckey[d][dst] = kk[u][d];
+          b.cidx[dst] = idv[u];
+        } else {
+          const int64_t dst = (c == 0u ? lBeg : rBeg) + rank;
+#pragma unroll
+          for (int d = 0; d < D; d++) b.key[nbuf][d][dst] = kk[u][d];
+          b.idx[nbuf][dst] = idv[u];
+          if (c == 0u) {
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+              lo[0][d] = min(lo[0][d], kk[u][d]);
+              hi[0][d] = max(hi[0][d], kk[u][d]);
+            }
+          } else {
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+              lo[1][d] = min(lo[1][d], kk[u][d]);
+              hi[1][d] = max(hi[1][d], kk[u][d]);
+            }
+          }
+        }
+      }
+      pos[0] += __popc(m0);
+      pos[1] += __popc(m1);
+      pos[2] += __popc(m2);
+    }
   }
   merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
 }
