@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-clouds", type=int, default=4096,
+                    help="clouds in the batched section (4096 = the configuration)")
     ap.add_argument("--configs", default="",
                     help="comma list of c1,c2,c4,c5: measure those configurations instead "
                          "(one JSON line each, not the benchmark line)")
@@ -338,7 +340,7 @@ def run_ours(args, rank, world, local):
                "d2h_bytes_per_step": int(h_ids.numel() * 4 + h_d2.numel() * 4),
                "ms_per_step": round(et / args.steps, 3)}
 
-    batched = None if args.no_batched else batched_section(ck, dev)
+    batched = None if args.no_batched else batched_section(ck, dev, args.batched_clouds)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -369,14 +371,14 @@ def run_ours(args, rank, world, local):
         print(json.dumps(out), flush=True)
 
 
-def batched_section(ck, dev):
+def batched_section(ck, dev, num_clouds=4096):
     """Many clouds built and queried together (cukd_batch_*): 4096 clouds of
     floor(exp(U[ln 256, ln 65536])) uniform points, 1024 uniform queries
     each, k = 8, stack-based; autotuned, then timed as CUDA-graph replays
     of build + query (the input cloud array is restored before each)."""
     import torch
     from cudakdtree_b200 import workloads as wl
-    pts, poff, qs, qoff = wl.batched_clouds()
+    pts, poff, qs, qoff = wl.batched_clouds(num_clouds=num_clouds)
     plan = ck.BatchPlan(poff, qoff, 3, k=8)
     src = torch.from_numpy(pts).to(dev)
     P = torch.empty_like(src)
@@ -410,7 +412,7 @@ def batched_section(ck, dev):
     query_ms = timed(lambda: plan.query(P, Q, bnd, out=out), 5)
     nq, n = qs.shape[0], pts.shape[0]
     del plan
-    return {"workload": "4096 clouds, sizes floor(exp(U[ln 256, ln 65536])) (seed 5), uniform "
+    return {"workload": f"{num_clouds} clouds, sizes floor(exp(U[ln 256, ln 65536])) (seed 5), uniform "
                         "points and 1024 uniform queries per cloud, float3, k=8, stack_based",
             "clouds": int(poff.size - 1), "points": int(n), "queries": int(nq), "k": 8,
             "tuning": {k: (round(v, 3) if isinstance(v, float) else v)
