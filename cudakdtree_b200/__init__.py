@@ -197,6 +197,9 @@ def lib():
         L.cukd_batch_query.argtypes = [C.c_void_p, P, P, P, P, P, P]
         L.cukd_batch_run.argtypes = [C.c_void_p, P, P, P, P, P, P]
         L.cukd_batch_autotune.argtypes = [C.c_void_p, P, P, C.c_int, C.POINTER(BatchTuning), P]
+        L.cukd_knn_accumulate.argtypes = [P, I64, C.POINTER(Layout), P, I64, P, I64, P, C.c_int,
+                                          C.c_float, C.c_int, P, P]
+        L.cukd_knn_lists_extract.argtypes = [P, I64, C.c_int, P, P, P, P]
         for name in ("cukd_build_float2", "cukd_build_float3", "cukd_build_float4",
                      "cukd_build_int2", "cukd_build_int3", "cukd_build_int4"):
             getattr(L, name).argtypes = [P, I64, P, P, P]

@@ -232,6 +232,32 @@ CUKD_API int cukd_morton_order(const float *d_points, int64_t n, int num_dims,
                       const cukd_mem_resource *mem);
 
 /* ------------------------------------------------------------------------
+ * Sharded kNN (reference: the ring of samples/mpiHugeQuery.cu:105-225, whose
+ * per-round kernel resumes a FlexHeapCandidateList, cukd/knn.h:360-371)
+ * ------------------------------------------------------------------------ */
+/* Folds one float tree shard (built by cukd_build_tree) into per-query
+ * candidate lists d_lists (device uint64[nq][k], ascending keys
+ * d2-float-bits << 32 | global id) that persist across calls; global id =
+ * node index + id_offset.  init != 0 starts each list as k slots of
+ * (max_radius^2, id 0xffffffff), the reference's round-0 list; otherwise the
+ * lists continue from the previous call.  After any sequence of calls a list
+ * holds the k smallest (d2, global id) keys over all points folded in, in any
+ * shard order.  d_order (optional) is a visiting order of the queries (for
+ * example cukd_morton_order's).  k = 1..128. */
+CUKD_API int cukd_knn_accumulate(const void *d_tree, int64_t n, const cukd_layout *layout,
+                                 const void *d_world_bounds, int64_t id_offset,
+                                 const void *d_queries, int64_t nq, const int32_t *d_order,
+                                 int k, float max_radius, int init, uint64_t *d_lists,
+                                 cudaStream_t stream);
+
+/* Splits lists into ids (-1 = unfilled), d2 ([nq][k] each, optional) and the
+ * k-th distance per query (optional; sqrt of the k-th d2 unless infinite,
+ * what mpiHugeQuery.cu's extractFinalResult writes, :77-90). */
+CUKD_API int cukd_knn_lists_extract(const uint64_t *d_lists, int64_t nq, int k,
+                                    int32_t *d_out_ids, float *d_out_d2, float *d_out_kth_dist,
+                                    cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
  * Spatial k-d tree (reference: cukd/spatial-kdtree.h)
  * ------------------------------------------------------------------------ */
 /* Node record, byte-identical to SpatialKDTree<>::Node
