@@ -6,6 +6,8 @@
 // with the CPU oracle.
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <fstream>
 #include <random>
 #include <string>
 #include <vector>
@@ -111,6 +113,22 @@ int main(int argc, char **argv)
   float3 *dq;
   CUKD_CUDA_CALL(Malloc(&dq, sizeof(float3) * nq));
   CUKD_CUDA_CALL(Memcpy(dq, qs.data(), sizeof(float3) * nq, cudaMemcpyHostToDevice));
+
+  // 0) point files: cukd::loadPoints reads the count + records layout
+  {
+    const std::string f = out + "/points_loadpoints.bin";
+    std::ofstream o(f, std::ios::binary);
+    const uint64_t cnt = uint64_t(n);
+    o.write(reinterpret_cast<const char *>(&cnt), sizeof(cnt));
+    o.write(reinterpret_cast<const char *>(pts.data()), sizeof(float3) * n);
+    o.close();
+    int count = 0;
+    float3 *lp = cukd::loadPoints<float3>(f, count);
+    if (count != n || memcmp(lp, pts.data(), sizeof(float3) * n) != 0)
+      throw std::runtime_error("loadPoints returned different records");
+    cudaFree(lp);
+    std::printf("loadPoints OK\n");
+  }
 
   // 1) README sample: point + payload, default builder, user kNN kernel
   {

@@ -24,6 +24,7 @@ def out(tmp_path_factory):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "shim_test OK" in r.stdout
     assert "sqrDist 2.8466301" in r.stdout
+    assert "loadPoints OK" in r.stdout
     return d
 
 
