@@ -42,6 +42,7 @@ METHODS = {"stack_based": STACK_BASED, "stackBased": STACK_BASED, "stack_free": 
            "stackFree": STACK_FREE, "cct": CCT}
 BUILDERS = {"default": 0, "thrust": 1, "bitonic": 2, "inplace": 3, "inPlace": 3}
 QUERY_MORTON, QUERY_HEAP_ORDER, QUERY_FORCE_HEAP, QUERY_REFERENCE_ORDER = 1, 2, 4, 8
+QUERY_TREE_ORDER = 16
 INT64_MAX = (1 << 63) - 1
 
 
@@ -277,7 +278,8 @@ def build_tree(points, layout=None, world_bounds=None, builder="default", stream
 
 
 def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True,
-            heap_order=False, force_heap=False, block_size=0, reference_order=False):
+            heap_order=False, force_heap=False, block_size=0, reference_order=False,
+            tree_order=False):
     p = QueryParams()
     p.method = METHODS[method] if isinstance(method, str) else int(method)
     p.k = k
@@ -286,14 +288,15 @@ def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=T
     p.cutoff_d2 = cutoff_d2
     p.flags = ((QUERY_MORTON if morton else 0) | (QUERY_HEAP_ORDER if heap_order else 0)
                | (QUERY_FORCE_HEAP if force_heap else 0)
-               | (QUERY_REFERENCE_ORDER if reference_order else 0))
+               | (QUERY_REFERENCE_ORDER if reference_order else 0)
+               | (QUERY_TREE_ORDER if tree_order else 0))
     p.block_size = block_size
     return p
 
 
 def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=None,
         cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True, with_d2=False,
-        stream=None, block_size=0, reference_order=False):
+        stream=None, block_size=0, reference_order=False, tree_order=False):
     """Find-closest-point for each query ([nq, D] tensor of the tree's scalar
     type).  Returns int32 node indices (-1 = none within the cut-off)."""
     layout = layout or infer_layout(tree)
@@ -306,7 +309,7 @@ def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=N
         d2 = torch.empty(nq, dtype=torch.float32 if layout.scalar_type == FLOAT32
                          else torch.int64, device=queries.device)
     p = _params(method, 1, cutoff, eps, cutoff_d2, morton, block_size=block_size,
-                reference_order=reference_order)
+                reference_order=reference_order, tree_order=tree_order)
     _check(lib().cukd_fcp(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
                           _ptr(queries.contiguous()), nq, C.byref(p), _ptr(ids), _ptr(d2),
                           _stream(stream), None), "cukd_fcp")
@@ -316,7 +319,7 @@ def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=N
 def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
         cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, heap_order=False,
         force_heap=False, with_max=False, stream=None, block_size=0, out_ids=None,
-        out_d2=None, reference_order=False, reordered_count=None):
+        out_d2=None, reference_order=False, reordered_count=None, tree_order=False):
     """k nearest neighbours.  Returns (ids [nq,k] int32, d2 [nq,k]) with the
     reference's candidate-list semantics; ascending unless heap_order."""
     layout = layout or infer_layout(tree)
@@ -329,7 +332,7 @@ def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, 
     d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, device=dev)
     mx = torch.empty(nq, dtype=dt, device=dev) if with_max else None
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton, heap_order, force_heap, block_size,
-                reference_order)
+                reference_order, tree_order)
     if reordered_count is not None:  # int32 CUDA tensor of one element
         p.d_reordered_count = reordered_count.data_ptr()
     _check(lib().cukd_knn(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "fast.cuh"
 #include "query.cuh"
+#include "sort.cuh"
 
 namespace ckb {
 namespace query {
@@ -52,6 +53,73 @@ __global__ void __launch_bounds__(256) query_kernel(QArgs a)
       trav_cct<SC, D>(res, q, rd, tv.n, (const T *)tv.bounds);
     res.write(a, qi);
   }
+}
+
+// Tree-path key of each query: the bits of the left / right choices of a
+// closest-side descent from the root to a leaf, left-aligned to the tree's
+// depth, so that sorting by it groups queries by the subtrees they enter
+// (an order adapted to this tree's splits; results are unchanged).
+template <int SC, int D, bool EXPL, bool VEC16>
+__global__ void __launch_bounds__(256) tree_path_kernel(QArgs a, int levels, uint32_t *codes,
+                                                        uint32_t *vals)
+{
+  using T = typename Traits<SC>::T;
+  const NodeReader<SC, D, EXPL, VEC16> rd(a);
+  const int N = int(a.n);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.nq;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    T q[D];
+    const T *qp = (const T *)a.queries + i * D;
+#pragma unroll
+    for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
+    uint32_t code = 0;
+    int depth = 0, curr = 0;
+    while (curr < N) {
+      T p[D];
+      const int dim = rd.load(curr, p);
+      T nodeC = p[0], queryC = q[0];
+#pragma unroll
+      for (int d = 1; d < D; d++)
+        if (d == dim) {
+          nodeC = p[d];
+          queryC = q[d];
+        }
+      const uint32_t right = queryC < nodeC ? 0u : 1u;
+      code = (code << 1) | right;
+      depth++;
+      curr = 2 * curr + 1 + int(right);
+    }
+    codes[i] = levels > depth ? code << (levels - depth) : code;
+    vals[i] = uint32_t(i);
+  }
+}
+
+template <int SC, int D, bool EXPL, bool VEC16>
+int launch_tree_path(const QArgs &a, int levels, uint32_t *codes, uint32_t *vals,
+                     cudaStream_t st)
+{
+  const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(div_up(a.nq, 256), kNumSMs * 16)));
+  tree_path_kernel<SC, D, EXPL, VEC16><<<blocks, 256, 0, st>>>(a, levels, codes, vals);
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+int run_tree_path(const QArgs &a, int scalar, int D, int levels, uint32_t *codes, uint32_t *vals,
+                  cudaStream_t st)
+{
+  const bool expl = a.doff >= 0;
+  const bool vec16 = a.stride == 16 && a.poff == 0 && (!expl || a.doff == 12) && D <= 3;
+#define CKB_TP(SC_, D_)                                                                   \
+  if (scalar == SC_ && D == D_) {                                                         \
+    if (expl) return vec16 ? launch_tree_path<SC_, D_, true, true>(a, levels, codes, vals, st) \
+                           : launch_tree_path<SC_, D_, true, false>(a, levels, codes, vals, st); \
+    return vec16 ? launch_tree_path<SC_, D_, false, true>(a, levels, codes, vals, st)      \
+                 : launch_tree_path<SC_, D_, false, false>(a, levels, codes, vals, st);    \
+  }
+  CKB_TP(0, 2) CKB_TP(0, 3) CKB_TP(0, 4)
+  CKB_TP(1, 2) CKB_TP(1, 3) CKB_TP(1, 4)
+#undef CKB_TP
+  return CUKD_ERR_UNSUPPORTED;
 }
 
 template <int SC, int D, bool EXPL, bool VEC16, int METHOD, class Res>
@@ -168,7 +236,17 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   a.visits = visits;
   a.block_size = p->block_size;
   TempArena arena(st, mem);
-  if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32) {
+  if ((p->flags & CUKD_QUERY_TREE_ORDER) && nq > 1 && n > 0) {
+    uint32_t *codes = nullptr, *codes2 = nullptr, *vals = nullptr, *vals2 = nullptr;
+    CKB_TRY(arena.alloc(&codes, nq));
+    CKB_TRY(arena.alloc(&codes2, nq));
+    CKB_TRY(arena.alloc(&vals, nq));
+    CKB_TRY(arena.alloc(&vals2, nq));
+    const int levels = num_levels(n);
+    CKB_TRY(run_tree_path(a, L.scalar, L.D, levels, codes, vals, st));
+    CKB_TRY(radix_sort_pairs(codes, vals, codes2, vals2, nq, levels, st, &arena));
+    a.order = (const int32_t *)vals;
+  } else if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32) {
     int32_t *perm = nullptr;
     CKB_TRY(arena.alloc(&perm, nq));
     CKB_TRY(morton_order_impl((const float *)d_queries, nq, L.D, nullptr, perm, st, mem));

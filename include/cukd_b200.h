@@ -179,7 +179,12 @@ enum {
    * queries whose answer cannot depend on the order -- no distance tie at
    * the k-th boundary -- take a faster traversal; the answers are the same
    * bits either way) */
-  CUKD_QUERY_REFERENCE_ORDER = 8
+  CUKD_QUERY_REFERENCE_ORDER = 8,
+  /* sort queries by the path a closest-side descent takes down this tree
+   * (left / right bits, root first) instead of by Morton code: an order
+   * adapted to the tree's own splits; results are unchanged.  Takes
+   * precedence over CUKD_QUERY_MORTON. */
+  CUKD_QUERY_TREE_ORDER = 16
 };
 
 typedef struct cukd_query_params {

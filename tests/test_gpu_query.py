@@ -183,3 +183,23 @@ def test_morton_order_is_a_permutation():
     q = make_queries(100003, 3, "gmm", seed=16)
     perm = ck.morton_order(torch.from_numpy(q).cuda()).cpu().numpy()
     assert np.array_equal(np.sort(perm), np.arange(len(q)))
+
+
+@pytest.mark.parametrize("kind", ["uniform", "tie", "gmm"])
+@pytest.mark.parametrize("explicit", [False, True])
+def test_tree_path_order_same_answers(kind, explicit):
+    """CUKD_QUERY_TREE_ORDER only changes the visiting order of the queries."""
+    n, nq = 20000, 8000
+    tree, dims, bounds = _tree(n, 3, kind, explicit, seed=11)
+    q = make_queries(nq, 3, kind, seed=12)
+    t, lay = _gpu_tree(tree, dims)
+    wb = torch.from_numpy(bounds).cuda()
+    dq = torch.from_numpy(q).cuda()
+    for k in (1, 16, 40):
+        ri, rd, _ = po.knn(tree, q, k, po.STACK_BASED, dims=dims, bounds=bounds)
+        ids, d2 = ck.knn(t, dq, k, "stack_based", layout=lay, world_bounds=wb, tree_order=True)
+        assert np.array_equal(ids.cpu().numpy(), ri)
+        assert np.array_equal(f32_bits(d2.cpu().numpy()), f32_bits(rd))
+    rf = po.fcp(tree, q, po.CCT, dims=dims, bounds=bounds)
+    assert np.array_equal(ck.fcp(t, dq, "cct", layout=lay, world_bounds=wb,
+                                 tree_order=True).cpu().numpy(), rf)
