@@ -254,8 +254,7 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   }
   // fast exact path (see fast.cu): any visiting order, boundary-tie check,
   // reference-order re-run of the queued queries
-  const bool fastOk = L.scalar == CUKD_FLOAT32 && !visits && !a.heap_order &&
-                      !(p->flags & CUKD_QUERY_REFERENCE_ORDER) &&
+  const bool fastOk = !visits && !a.heap_order && !(p->flags & CUKD_QUERY_REFERENCE_ORDER) &&
                       knn && p->k >= 2 && p->k <= 128 && n < (int64_t(1) << 31) - 1;
   // (FCP and k = 1 stay on the reference traversals: with a single
   // candidate the split-plane bound is already cheap and the corner
@@ -271,7 +270,7 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
     fa.work = ctr;
     fa.fb_count = ctr + 1;
     CKB_TRY(arena.alloc(&fa.fb_list, nq));
-    CKB_TRY(run_fast(fa, L.D, st));
+    CKB_TRY(L.scalar == CUKD_FLOAT32 ? run_fast(fa, L.D, st) : run_fast_int(fa, L.D, st));
     if (p->d_reordered_count)
       CKB_CUDA(cudaMemcpyAsync(p->d_reordered_count, fa.fb_count, sizeof(int),
                                cudaMemcpyDeviceToDevice, st));

@@ -118,7 +118,7 @@ def test_knn_dims_cutoff(mname, m, explicit, D, cutoff, k):
 
 
 @pytest.mark.parametrize("mname,m", METHODS)
-@pytest.mark.parametrize("k", [1, 8, 64])
+@pytest.mark.parametrize("k", [1, 2, 8, 16, 33, 64, 128])
 @pytest.mark.parametrize("explicit", [False, True])
 def test_int_coordinates(mname, m, k, explicit):
     """int32 trees: exact int64 squared distances (no reference traversal
@@ -203,3 +203,21 @@ def test_tree_path_order_same_answers(kind, explicit):
     rf = po.fcp(tree, q, po.CCT, dims=dims, bounds=bounds)
     assert np.array_equal(ck.fcp(t, dq, "cct", layout=lay, world_bounds=wb,
                                  tree_order=True).cpu().numpy(), rf)
+
+
+@pytest.mark.parametrize("mname,m", METHODS)
+@pytest.mark.parametrize("k", [4, 16, 64])
+@pytest.mark.parametrize("cutoff_d2", [2**62, 40, 0])
+def test_int_tie_heavy_and_cutoff(mname, m, k, cutoff_d2):
+    """Integer fast path on tie-heavy points (many equal distances at the
+    k-th boundary, re-run in the reference order) with squared cut-offs,
+    including a point exactly at the cut-off."""
+    n, nq = 20000, 6000
+    tree, dims, bounds = _tree(n, 3, "tie", False, scalar="int32", seed=13)
+    q = make_queries(nq, 3, "tie", scalar="int32", seed=14)
+    ri, rd, _ = po.knn(tree, q, k, m, bounds=bounds, cutoff_d2_int=cutoff_d2)
+    t, lay = _gpu_tree(tree, dims)
+    ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), k, mname, layout=lay,
+                     world_bounds=torch.from_numpy(bounds).cuda(), cutoff_d2=cutoff_d2)
+    assert np.array_equal(ids.cpu().numpy(), ri)
+    assert np.array_equal(d2.cpu().numpy(), rd)
