@@ -76,7 +76,11 @@ const char *last_cuda_error_string() { return cudaGetErrorString(g_last_cuda); }
 namespace build {
 
 constexpr int kTile = 2048;       // max subtree size finished in shared memory
-constexpr int kSubThreads = 256;  // threads of the subtree CTA
+// threads of a subtree CTA: 512 (two resident CTAs per SM, 64 registers) for
+// the single tree's 2048-point subtrees, 256 for the forest's tile classes,
+// whichever measured faster
+constexpr int kSubThreads = 256;
+constexpr int kSubThreadsTree = 512;
 constexpr int kChunk = 4096;      // points per CTA in hist / partition
 constexpr int kGThreads = 256;
 constexpr int kMaxBins = 4096;
@@ -677,7 +681,7 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
 // ---------------------------------------------------------------------------
 // subtree phase: one CTA per subtree of <= kTile points
 // ---------------------------------------------------------------------------
-template <int D, int TILE>
+template <int D, int TILE, int NT>
 struct SubSmem {
   uint32_t key[D][TILE];
   uint32_t idx[TILE];
@@ -685,18 +689,18 @@ struct SubSmem {
   uint16_t segOf[2][TILE];
   union {
     uint32_t scan[TILE];                 // level partitions
-    uint16_t rh[kSubThreads / 32][256];  // presort: per-warp digit counts / offsets
+    uint16_t rh[NT / 32][256];  // presort: per-warp digit counts / offsets
   };
   struct {
     uint16_t t0[TILE], t1[TILE], b[TILE], r[TILE];
   } u_sub;
-  uint32_t red[2 * (kSubThreads / 32)];
+  uint32_t red[2 * (NT / 32)];
   uint16_t locPivot[2 * TILE];
   uint8_t locDim[2 * TILE];
   uint8_t flag[TILE];
   uint8_t subDim[TILE];
   uint16_t queue[TILE];
-  uint32_t warpSums[kSubThreads / 32];
+  uint32_t warpSums[NT / 32];
   uint32_t qcount;
   uint32_t rootLo[D], rootHi[D];
 };
@@ -706,14 +710,15 @@ struct SubSmem {
 // owns a contiguous run of positions; match_any ranks equal digits inside a
 // round of 32, per-warp digit counts scanned digit-major order the warps.
 // Result in `a`; `tmp` is scratch of m entries.
+template <int NT>
 __device__ void sub_radix_sort(const uint32_t *__restrict__ key, int m, uint16_t *a,
                                uint16_t *tmp, uint16_t (*rh)[256], uint32_t *red)
 {
-  constexpr int W = kSubThreads / 32;
-  static_assert(kSubThreads == 256, "one thread per digit in the scan");
+  constexpr int W = NT / 32;
+  static_assert(NT >= 256 && NT % 256 == 0, "a thread per digit in the scan");
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   uint32_t lo = 0xffffffffu, hi = 0u;
-  for (int i = tid; i < m; i += kSubThreads) {
+  for (int i = tid; i < m; i += NT) {
     const uint32_t k = key[i];
     lo = min(lo, k);
     hi = max(hi, k);
@@ -744,7 +749,7 @@ __device__ void sub_radix_sort(const uint32_t *__restrict__ key, int m, uint16_t
   uint16_t *src = a, *dst = tmp;
   for (int ps = 0; ps < passes; ps++) {
     const int shift = ps * 8;
-    for (int i = tid; i < W * 256; i += kSubThreads) (&rh[0][0])[i] = 0;
+    for (int i = tid; i < W * 256; i += NT) (&rh[0][0])[i] = 0;
     __syncthreads();
     for (int base = w0; base < w1; base += 32) {
       const int i = base + lane;
@@ -755,26 +760,30 @@ __device__ void sub_radix_sort(const uint32_t *__restrict__ key, int m, uint16_t
     }
     __syncthreads();
     {
-      // digit-major exclusive offsets: thread = digit
-      uint32_t run = 0;
+      // digit-major exclusive offsets: threads 0..255 own one digit each
+      uint32_t run = 0, incl = 0;
+      if (tid < 256) {
 #pragma unroll
-      for (int w = 0; w < W; w++) {
-        const uint32_t c = rh[w][tid];
-        rh[w][tid] = uint16_t(run);
-        run += c;
+        for (int w = 0; w < W; w++) {
+          const uint32_t c = rh[w][tid];
+          rh[w][tid] = uint16_t(run);
+          run += c;
+        }
+        incl = run;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        if (lane == 31) red[wid] = incl;
       }
-      uint32_t incl = run;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      if (lane == 31) red[wid] = incl;
       __syncthreads();
-      uint32_t wbase = 0;
-      for (int w = 0; w < wid; w++) wbase += red[w];
-      const uint32_t dbase = wbase + incl - run;
+      if (tid < 256) {
+        uint32_t wbase = 0;
+        for (int w = 0; w < wid; w++) wbase += red[w];
+        const uint32_t dbase = wbase + incl - run;
 #pragma unroll
-      for (int w = 0; w < W; w++) rh[w][tid] = uint16_t(rh[w][tid] + dbase);
+        for (int w = 0; w < W; w++) rh[w][tid] = uint16_t(rh[w][tid] + dbase);
+      }
     }
     __syncthreads();
     for (int base = w0; base < w1; base += 32) {
@@ -797,7 +806,7 @@ __device__ void sub_radix_sort(const uint32_t *__restrict__ key, int m, uint16_t
     dst = t;
   }
   if (src != a) {
-    for (int i = tid; i < m; i += kSubThreads) a[i] = src[i];
+    for (int i = tid; i < m; i += NT) a[i] = src[i];
     __syncthreads();
   }
 }
@@ -805,16 +814,16 @@ __device__ void sub_radix_sort(const uint32_t *__restrict__ key, int m, uint16_t
 // Finishes the subtree under node s (level L0) of a tree of n records whose
 // first record sits at `base` of the working arrays; `boxIndex` selects the
 // subtree's domain box in b.sbox[0] (explicit dims only).
-template <int SC, int D, int TILE>
+template <int SC, int D, int TILE, int NT>
 __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_t base,
-                             int64_t boxIndex, int cb, bool explicitDims, SubSmem<D, TILE> &S)
+                             int64_t boxIndex, int cb, bool explicitDims, SubSmem<D, TILE, NT> &S)
 {
   const int tid = threadIdx.x;
   const int64_t sb = base + seg_begin(s, L0, n);
   const int m = int(subtree_size(s, n));
   if (m == 0) return;
 
-  for (int i = tid; i < m; i += kSubThreads) {
+  for (int i = tid; i < m; i += NT) {
 #pragma unroll
     for (int d = 0; d < D; d++) S.key[d][i] = b.key[cb][d][sb + i];
     S.idx[i] = b.idx[cb][sb + i];
@@ -828,7 +837,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
 
   // one coordinate-sorted index list per dimension (equal keys in any
   // order; runs of equal keys are ranked by the composite key below)
-  for (int d = 0; d < D; d++) sub_radix_sort(S.key[d], m, S.list[0][d], S.list[1][d], S.rh, S.red);
+  for (int d = 0; d < D; d++) sub_radix_sort<NT>(S.key[d], m, S.list[0][d], S.list[1][d], S.rh, S.red);
 
   int cur = 0;
   int mact = m;
@@ -842,7 +851,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     if (tid == 0) S.qcount = 0;
     __syncthreads();
     // A: per subtree, its dim, pivot rank position and equal-key run
-    for (int t = tid; t < nexist; t += kSubThreads) {
+    for (int t = tid; t < nexist; t += NT) {
       const int64_t g = g0 + t;
       const int sz = int(subtree_size(g, n));
       const int bt = int(seg_begin(g, lvl, n) - base0);
@@ -911,7 +920,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     }
     __syncthreads();
     // A2: rank equal-coordinate runs by the composite key (one warp each)
-    for (int qi = wid; qi < int(S.qcount); qi += kSubThreads / 32) {
+    for (int qi = wid; qi < int(S.qcount); qi += NT / 32) {
       const int t = S.queue[qi];
       const int64_t g = g0 + t;
       const int u = (1 << j) - 1 + t;
@@ -971,7 +980,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     }
     __syncthreads();
     // B: sides of all points outside the runs
-    for (int p = tid; p < mact; p += kSubThreads) {
+    for (int p = tid; p < mact; p += NT) {
       const int t = S.segOf[cur][p];
       const int e = S.list[cur][S.subDim[t]][p];
       if (p < S.u_sub.t0[t])
@@ -981,7 +990,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     }
     __syncthreads();
     // C: stable partition of every list (pivots dropped)
-    constexpr int PER = TILE / kSubThreads;
+    constexpr int PER = TILE / NT;
     for (int d = 0; d < D; d++) {
       const uint16_t *Lc = S.list[cur][d];
       uint32_t local = 0;
@@ -1014,7 +1023,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
         }
       }
       __syncthreads();
-      for (int p = tid; p < mact; p += kSubThreads) {
+      for (int p = tid; p < mact; p += NT) {
         const int e = Lc[p];
         const int f = S.flag[e];
         if (f == 2) continue;
@@ -1035,13 +1044,14 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
 }
 
 template <int SC, int D>
-__global__ void __launch_bounds__(kSubThreads) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
+__global__ void __launch_bounds__(kSubThreadsTree, 2) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
                                                               bool explicitDims)
 {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  SubSmem<D, kTile> &S = *reinterpret_cast<SubSmem<D, kTile> *>(smem_raw);
+  SubSmem<D, kTile, kSubThreadsTree> &S =
+      *reinterpret_cast<SubSmem<D, kTile, kSubThreadsTree> *>(smem_raw);
   const int seg = blockIdx.x;
-  subtree_body<SC, D, kTile>(b, n, L0, ((int64_t(1) << L0) - 1) + seg, 0, seg, cb, explicitDims,
+  subtree_body<SC, D, kTile, kSubThreadsTree>(b, n, L0, ((int64_t(1) << L0) - 1) + seg, 0, seg, cb, explicitDims,
                              S);
 }
 
@@ -1053,7 +1063,7 @@ template <int D, int TILE>
 __global__ void __launch_bounds__(kSubThreads) subtree_forest_kernel(Bufs b, ForestSubtrees f)
 {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  SubSmem<D, TILE> &S = *reinterpret_cast<SubSmem<D, TILE> *>(smem_raw);
+  SubSmem<D, TILE, kSubThreads> &S = *reinterpret_cast<SubSmem<D, TILE, kSubThreads> *>(smem_raw);
   __shared__ int next;
   for (;;) {
     if (threadIdx.x == 0) next = atomicAdd(f.counter, 1);
@@ -1063,7 +1073,7 @@ __global__ void __launch_bounds__(kSubThreads) subtree_forest_kernel(Bufs b, For
     if (w >= f.items) break;
     const int c = f.cloud[w];
     const int L0 = f.level[w];
-    subtree_body<0, D, TILE>(b, f.cloudN[c], L0, ((int64_t(1) << L0) - 1) + f.local[w],
+    subtree_body<0, D, TILE, kSubThreads>(b, f.cloudN[c], L0, ((int64_t(1) << L0) - 1) + f.local[w],
                              f.cloudBase[c], -1, L0 & 1, false, S);
     __syncthreads();
   }
@@ -1186,10 +1196,10 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
     std::swap(b.sbox[0], b.sbox[1]);
   }
   {
-    const size_t smem = sizeof(SubSmem<D, kTile>);
+    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreadsTree>);
     CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
+    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreadsTree, smem, st>>>(b, n, G, cb,
                                                                        explicitDims);
     CKB_CHECK_LAUNCH();
   }
@@ -1405,10 +1415,10 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
     std::swap(b.sbox[0], b.sbox[1]);
   }
   {
-    const size_t smem = sizeof(SubSmem<D, kTile>);
+    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreadsTree>);
     CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
+    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreadsTree, smem, st>>>(b, n, G, cb,
                                                                        explicitDims);
     CKB_CHECK_LAUNCH();
   }
@@ -1566,7 +1576,7 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
     // (the shared-memory opt-in was made by forest_subtree_occupancy)
 #define CKB_SUB(T_)                                                                 \
   if (kForestTiles[c] == T_) {                                                      \
-    subtree_forest_kernel<D, T_><<<grid, kSubThreads, sizeof(SubSmem<D, T_>), s>>>(b, S); \
+    subtree_forest_kernel<D, T_><<<grid, kSubThreads, sizeof(SubSmem<D, T_, kSubThreads>), s>>>(b, S); \
     CKB_CHECK_LAUNCH();                                                             \
   }
     CKB_SUB(512) CKB_SUB(1024) CKB_SUB(2048)
@@ -1589,7 +1599,7 @@ template <int D, int T>
 int subtree_occupancy()
 {
   int blocks = 0;
-  const size_t smem = sizeof(SubSmem<D, T>);
+  const size_t smem = sizeof(SubSmem<D, T, kSubThreads>);
   if (cudaFuncSetAttribute(subtree_forest_kernel<D, T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, subtree_forest_kernel<D, T>,
