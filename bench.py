@@ -297,7 +297,7 @@ def run_ours(args, rank, world, local):
     achieved = knn_bytes / (knn_sb_ms / 1e3) / 1e9
     traffic = profile_traffic("knn_stack_based_k16_10M")
     roofline = {"bound": "hbm", "kernel": "knn stack-based k=16 (cukd_knn: Morton order + "
-                "query_kernel)", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "knn_fast_kernel + reference-order re-run of tied queries)", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "algorithmic_bytes": knn_bytes,
                 "bytes_formula": "sum(visits_ref)*16 + nq*12 + nq*k*8",
