@@ -198,6 +198,8 @@ def lib():
         L.cukd_batch_query.argtypes = [C.c_void_p, P, P, P, P, P, P]
         L.cukd_batch_run.argtypes = [C.c_void_p, P, P, P, P, P, P]
         L.cukd_batch_autotune.argtypes = [C.c_void_p, P, P, C.c_int, C.POINTER(BatchTuning), P]
+        L.cukd_knn_host.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
+                                    C.POINTER(QueryParams), P, P, I64, P, P]
         L.cukd_knn_accumulate.argtypes = [P, I64, C.POINTER(Layout), P, I64, P, I64, P, C.c_int,
                                           C.c_float, C.c_int, P, P]
         L.cukd_knn_lists_extract.argtypes = [P, I64, C.c_int, P, P, P, P]
@@ -339,6 +341,31 @@ def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, 
                           _ptr(queries.contiguous()), nq, C.byref(p), _ptr(ids), _ptr(d2),
                           _ptr(mx), _stream(stream), None), "cukd_knn")
     return (ids, d2, mx) if with_max else (ids, d2)
+
+
+def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
+             cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, out_ids=None, out_d2=None,
+             chunk=0, stream=None):
+    """knn() with host-resident queries and results (CPU tensors; pin them
+    for the copies to overlap the search).  Returns (ids, d2) CPU tensors,
+    complete once ``stream`` (default: the current stream) is synchronised."""
+    layout = layout or infer_layout(tree)
+    if n is None:
+        n = _num_records(tree, layout)
+    if queries.is_cuda:
+        raise ValueError("queries must be host memory (use knn() for device queries)")
+    nq = queries.shape[0]
+    queries = queries.contiguous()
+    dt = torch.float32 if layout.scalar_type == FLOAT32 else torch.int64
+    pin = queries.is_pinned()
+    ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32,
+                                                          pin_memory=pin)
+    d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, pin_memory=pin)
+    p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
+    _check(lib().cukd_knn_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds), _ptr(queries),
+                               nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk), _stream(stream),
+                               None), "cukd_knn_host")
+    return ids, d2
 
 
 def knn_visits(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,

@@ -223,6 +223,18 @@ CUKD_API int cukd_knn(const void *d_tree, int64_t n, const cukd_layout *layout,
              const cukd_query_params *params, int32_t *d_out_ids, void *d_out_d2,
              void *d_out_max_d2, cudaStream_t stream, const cukd_mem_resource *mem);
 
+/* cukd_knn with the queries and results in host memory: the queries are
+ * processed in chunks of `chunk` (0 = 2^20) whose host->device copies,
+ * searches and device->host copies overlap on three streams.  Results are
+ * cukd_knn's.  Use page-locked host buffers (cudaHostAlloc) for the copies
+ * to overlap.  Returns once the work is queued; `stream` completes after the
+ * last result copy.  No reference counterpart as one call (the reference's
+ * samples copy whole arrays around one query launch, sample.cu:121-160). */
+CUKD_API int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *layout,
+                           const void *d_world_bounds, const void *h_queries, int64_t nq,
+                           const cukd_query_params *params, int32_t *h_out_ids, void *h_out_d2,
+                           int64_t chunk, cudaStream_t stream, const cukd_mem_resource *mem);
+
 /* Per-query visited-node counts of the same traversal (the reference's
  * CUKD_ENABLE_STATS counter, cukd/common.h:345-360, per query). */
 CUKD_API int cukd_knn_visits(const void *d_tree, int64_t n, const cukd_layout *layout,
