@@ -1059,11 +1059,19 @@ __global__ void __launch_bounds__(kSubThreadsTree, 2) subtree_kernel(Bufs b, int
 // work item from a global counter until the list (sorted by size, largest
 // first) is exhausted.  A tree whose top-down phase ran L0 levels left its
 // records in key buffer L0 & 1.  Round-robin split dims.
+// threads per CTA of a tile class: 512 for 2048-point subtrees (as the single
+// tree's), 256 below (more resident CTAs; measured faster for those classes)
+template <int TILE> struct ForestNT {
+  static constexpr int value = TILE == 2048 ? kSubThreadsTree : kSubThreads;
+};
+
 template <int D, int TILE>
-__global__ void __launch_bounds__(kSubThreads) subtree_forest_kernel(Bufs b, ForestSubtrees f)
+__global__ void __launch_bounds__(ForestNT<TILE>::value, (ForestNT<TILE>::value > 256 ? 2 : 1))
+    subtree_forest_kernel(Bufs b, ForestSubtrees f)
 {
+  constexpr int NT = ForestNT<TILE>::value;
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  SubSmem<D, TILE, kSubThreads> &S = *reinterpret_cast<SubSmem<D, TILE, kSubThreads> *>(smem_raw);
+  SubSmem<D, TILE, NT> &S = *reinterpret_cast<SubSmem<D, TILE, NT> *>(smem_raw);
   __shared__ int next;
   for (;;) {
     if (threadIdx.x == 0) next = atomicAdd(f.counter, 1);
@@ -1073,7 +1081,7 @@ __global__ void __launch_bounds__(kSubThreads) subtree_forest_kernel(Bufs b, For
     if (w >= f.items) break;
     const int c = f.cloud[w];
     const int L0 = f.level[w];
-    subtree_body<0, D, TILE, kSubThreads>(b, f.cloudN[c], L0, ((int64_t(1) << L0) - 1) + f.local[w],
+    subtree_body<0, D, TILE, NT>(b, f.cloudN[c], L0, ((int64_t(1) << L0) - 1) + f.local[w],
                              f.cloudBase[c], -1, L0 & 1, false, S);
     __syncthreads();
   }
@@ -1576,7 +1584,8 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
     // (the shared-memory opt-in was made by forest_subtree_occupancy)
 #define CKB_SUB(T_)                                                                 \
   if (kForestTiles[c] == T_) {                                                      \
-    subtree_forest_kernel<D, T_><<<grid, kSubThreads, sizeof(SubSmem<D, T_, kSubThreads>), s>>>(b, S); \
+    subtree_forest_kernel<D, T_><<<grid, ForestNT<T_>::value,                       \
+                                   sizeof(SubSmem<D, T_, ForestNT<T_>::value>), s>>>(b, S); \
     CKB_CHECK_LAUNCH();                                                             \
   }
     CKB_SUB(512) CKB_SUB(1024) CKB_SUB(2048)
@@ -1599,11 +1608,11 @@ template <int D, int T>
 int subtree_occupancy()
 {
   int blocks = 0;
-  const size_t smem = sizeof(SubSmem<D, T, kSubThreads>);
+  const size_t smem = sizeof(SubSmem<D, T, ForestNT<T>::value>);
   if (cudaFuncSetAttribute(subtree_forest_kernel<D, T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, subtree_forest_kernel<D, T>,
-                                                    kSubThreads, smem) != cudaSuccess) {
+                                                    ForestNT<T>::value, smem) != cudaSuccess) {
     cudaGetLastError();
     return 1;
   }
