@@ -77,7 +77,7 @@ namespace build {
 
 constexpr int kTile = 2048;       // max subtree size finished in shared memory
 // threads of a subtree CTA: 512 (two resident CTAs per SM, 64 registers) for
-// the single tree's 2048-point subtrees, 256 for the forest's tile classes,
+// 2048-point subtrees, 256 for the forest's 512- and 1024-point tile classes,
 // whichever measured faster
 constexpr int kSubThreads = 256;
 constexpr int kSubThreadsTree = 512;
