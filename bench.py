@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-clouds", type=int, default=4096,
                     help="clouds in the batched section (4096 = the configuration)")
+    ap.add_argument("--batched-tuning", default="",
+                    help="tile,block,queries_per_thread,morton for the batched section "
+                         "instead of autotuning (profiling runs)")
     ap.add_argument("--e2e-chunk", type=int, default=1 << 21,
                     help="queries per chunk of the host-buffer kNN in the e2e measurement")
     ap.add_argument("--configs", default="",
@@ -343,7 +346,8 @@ def run_ours(args, rank, world, local):
                "api": (f"cukd_build_tree + cukd_knn_host (pinned host queries and results, "
                        f"{args.e2e_chunk}-query chunks on overlapping copy / search streams)")}
 
-    batched = None if args.no_batched else batched_section(ck, dev, args.batched_clouds)
+    batched = None if args.no_batched else batched_section(ck, dev, args.batched_clouds,
+                                                           args.batched_tuning)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -374,7 +378,7 @@ def run_ours(args, rank, world, local):
         print(json.dumps(out), flush=True)
 
 
-def batched_section(ck, dev, num_clouds=4096):
+def batched_section(ck, dev, num_clouds=4096, tuning=""):
     """Many clouds built and queried together (cukd_batch_*): 4096 clouds of
     floor(exp(U[ln 256, ln 65536])) uniform points, 1024 uniform queries
     each, k = 8, stack-based; autotuned, then timed as CUDA-graph replays
@@ -388,7 +392,12 @@ def batched_section(ck, dev, num_clouds=4096):
     Q = torch.from_numpy(qs).to(dev)
     bnd = plan.bounds_tensor(dev)
     out = plan._outputs(dev)
-    tune = plan.autotune(src, Q, reps=3)
+    if tuning:
+        t, bs, qpt, mo = (int(v) for v in tuning.split(","))
+        plan.set_tuning(build_tile=t, block_size=bs, queries_per_thread=qpt, morton=mo)
+        tune = plan.tuning
+    else:
+        tune = plan.autotune(src, Q, reps=3)
 
     def run():
         P.copy_(src, non_blocking=True)
