@@ -75,6 +75,7 @@ const char *last_cuda_error_string() { return cudaGetErrorString(g_last_cuda); }
 
 namespace build {
 
+constexpr int ilog2_floor(int x) { return x <= 1 ? 0 : 1 + ilog2_floor(x >> 1); }
 constexpr int kTile = 2048;       // max subtree size finished in shared memory
 // threads of a subtree CTA: 512 (two resident CTAs per SM, 64 registers) for
 // 2048-point subtrees, 256 for the forest's 512- and 1024-point tile classes,
@@ -688,7 +689,7 @@ struct SubSmem {
   uint16_t list[2][D][TILE];
   uint16_t segOf[2][TILE];
   union {
-    uint32_t scan[TILE];                 // level partitions
+    uint32_t scan[TILE];        // level partitions: per-subtree offsets
     uint16_t rh[NT / 32][256];  // presort: per-warp digit counts / offsets
   };
   struct {
@@ -700,8 +701,8 @@ struct SubSmem {
   uint8_t flag[TILE];
   uint8_t subDim[TILE];
   uint16_t queue[TILE];
-  uint32_t warpSums[NT / 32];
-  uint32_t qcount;
+  uint32_t warpSums[TILE / 32];  // partitions: per (round, warp) side counts
+  uint32_t qcount[2];  // run queue length, by level parity
   uint32_t rootLo[D], rootHi[D];
 };
 
@@ -829,6 +830,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     S.idx[i] = b.idx[cb][sb + i];
     S.segOf[0][i] = 0;
   }
+  if (tid < 2) S.qcount[tid] = 0;
   if (tid < D && boxIndex >= 0) {
     S.rootLo[tid] = b.sbox[0][boxIndex * 2 * D + tid];
     S.rootHi[tid] = b.sbox[0][boxIndex * 2 * D + D + tid];
@@ -848,8 +850,8 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
     const int64_t base0 = seg_begin(g0, lvl, n);
     const int nsub = 1 << j;
     int nexist = int(min(int64_t(nsub), max(int64_t(0), n - g0)));
-    if (tid == 0) S.qcount = 0;
-    __syncthreads();
+    uint32_t &qcount = S.qcount[j & 1];
+    if (tid == 0) S.qcount[(j + 1) & 1] = 0;  // the next level's; read last a level ago
     // A: per subtree, its dim, pivot rank position and equal-key run
     for (int t = tid; t < nexist; t += NT) {
       const int64_t g = g0 + t;
@@ -865,15 +867,22 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
           lo[d] = S.rootLo[d];
           hi[d] = S.rootHi[d];
         }
-        for (int c = u; c > 0;) {
-          const int p = (c - 1) >> 1;
-          const int pd = S.locDim[p];
-          const uint32_t pc = S.key[pd][S.locPivot[p]];
-          if (c & 1)
-            hi[pd] = min(hi[pd], pc);
-          else
-            lo[pd] = max(lo[pd], pc);
-          c = p;
+        // the a-th ancestor of local node u is ((u + 1) >> a) - 1; its loads
+        // do not depend on the nearer ancestors', so they issue together
+        constexpr int kMaxDepth = ilog2_floor(TILE);
+#pragma unroll
+        for (int a = 1; a <= kMaxDepth; a++) {
+          const bool on = a <= j;
+          const int c = on ? ((u + 1) >> (a - 1)) - 1 : 0;
+          const int p = on ? ((u + 1) >> a) - 1 : 0;
+          const int pd = on ? int(S.locDim[p]) : 0;
+          const uint32_t pc = S.key[pd][on ? int(S.locPivot[p]) : 0];
+          if (on) {
+            if (c & 1)
+              hi[pd] = min(hi[pd], pc);
+            else
+              lo[pd] = max(lo[pd], pc);
+          }
         }
         dim = Scalar<SC>::widest(lo, hi, D);
       } else {
@@ -884,7 +893,11 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
       const uint32_t *Kd = S.key[dim];
       const int pp = bt + r;
       const uint32_t v = Kd[Ld[pp]];
+      // neighbours first: a run of one (distinct keys) needs no search
+      const bool lone0 = pp == bt || Kd[Ld[pp - 1]] < v;
+      const bool lone1 = pp + 1 == bt + sz || Kd[Ld[pp + 1]] > v;
       int lo = bt, hi = pp;  // first q in [bt,pp] with key >= v
+      if (lone0) lo = pp;
       while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (Kd[Ld[mid]] < v)
@@ -895,6 +908,7 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
       const int t0 = lo;
       lo = pp + 1;
       hi = bt + sz;  // first q in [pp+1, bt+sz) with key > v
+      if (lone1) hi = lo;
       while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (Kd[Ld[mid]] <= v)
@@ -915,12 +929,44 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
         b.perm[base + g] = S.idx[piv];
         b.ndim[base + g] = uint8_t(dim);
       } else {
-        S.queue[atomicAdd(&S.qcount, 1u)] = uint16_t(t);
+        S.queue[atomicAdd(&qcount, 1u)] = uint16_t(t);
       }
     }
     __syncthreads();
-    // A2: rank equal-coordinate runs by the composite key (one warp each)
-    for (int qi = wid; qi < int(S.qcount); qi += NT / 32) {
+    // Thread tid owns the positions q*NT + tid (round q < PER) of the level;
+    // each position's subtree and whether it is its subtree's first position
+    // stay in registers for B and C.
+    constexpr int PER = TILE / NT;
+    constexpr int NW = NT / 32;
+    constexpr int NE = PER * NW;  // (round, warp) pairs, in position order
+    static_assert(PER >= 1 && NE <= 64, "one to two (round, warp) pairs per lane");
+    uint16_t tq[PER];
+    uint32_t startMask = 0;
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      const int p = q * NT + tid;
+      tq[q] = 0;
+      if (p < mact) {
+        tq[q] = S.segOf[cur][p];
+        if (p == 0 || S.segOf[cur][p - 1] != tq[q]) startMask |= 1u << q;
+      }
+    }
+    // B: sides of all points outside the runs
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      const int p = q * NT + tid;
+      if (p < mact) {
+        const int t = tq[q];
+        const int e = S.list[cur][S.subDim[t]][p];
+        if (p < S.u_sub.t0[t])
+          S.flag[e] = 0;
+        else if (p >= S.u_sub.t1[t])
+          S.flag[e] = 1;
+      }
+    }
+    // A2: rank equal-coordinate runs by the composite key (one warp each;
+    // the points of runs and those B flags are disjoint)
+    for (int qi = wid; qi < int(qcount); qi += NT / 32) {
       const int t = S.queue[qi];
       const int64_t g = g0 + t;
       const int u = (1 << j) - 1 + t;
@@ -979,65 +1025,80 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
       }
     }
     __syncthreads();
-    // B: sides of all points outside the runs
-    for (int p = tid; p < mact; p += NT) {
-      const int t = S.segOf[cur][p];
-      const int e = S.list[cur][S.subDim[t]][p];
-      if (p < S.u_sub.t0[t])
-        S.flag[e] = 0;
-      else if (p >= S.u_sub.t1[t])
-        S.flag[e] = 1;
+    // C: stable partition of every list (pivots dropped).  Sides are warp
+    // ballots, so a count of left / right points before a position is a
+    // popc plus the exclusive scan of the per-(round, warp) counts; the low /
+    // high 16 bits of a count word hold the two sides.  Each subtree's first
+    // position stores in pack[t] the offsets that turn those counts into new
+    // positions (pack aliases `scan`, free here).  List d+1 is counted in
+    // the phase that scatters list d.
+    const uint32_t ltMask = (1u << lane) - 1u;
+    uint32_t *pack = S.scan;
+    uint16_t eq[PER];
+    uint32_t bl[PER], br[PER];
+    auto count_sides = [&](int d) {
+      const uint16_t *Lc = S.list[cur][d];
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int p = q * NT + tid;
+        int f = 2;
+        eq[q] = 0;
+        if (p < mact) {
+          eq[q] = Lc[p];
+          f = S.flag[eq[q]];
+        }
+        bl[q] = __ballot_sync(0xffffffffu, f == 0);
+        br[q] = __ballot_sync(0xffffffffu, f == 1);
+        if (lane == 0) S.warpSums[q * NW + wid] = uint32_t(__popc(bl[q])) | (uint32_t(__popc(br[q])) << 16);
+      }
+    };
+    count_sides(0);
+    for (int d = 0; d < D; d++) {
+      __syncthreads();
+      // exclusive scan of the NE pair counts, two per lane
+      const uint32_t a0 = 2 * lane < NE ? S.warpSums[2 * lane] : 0u;
+      const uint32_t a1 = 2 * lane + 1 < NE ? S.warpSums[2 * lane + 1] : 0u;
+      uint32_t incl = a0 + a1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t excl = incl - a0 - a1;
+      uint32_t bef[PER];
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int ei = q * NW + wid;
+        const uint32_t x = __shfl_sync(0xffffffffu, excl, ei >> 1);
+        const uint32_t y = __shfl_sync(0xffffffffu, a0, ei >> 1);
+        bef[q] = x + ((ei & 1) ? y : 0u) +
+                 (uint32_t(__popc(bl[q] & ltMask)) | (uint32_t(__popc(br[q] & ltMask)) << 16));
+        if ((startMask >> q) & 1u) {
+          const int t = tq[q];
+          const int nb = q * NT + tid - t;  // first new position of subtree t
+          const int lb = nb - int(bef[q] & 0xffffu);
+          const int rb = nb + S.u_sub.r[t] - int(bef[q] >> 16);
+          pack[t] = uint32_t(uint16_t(lb)) | (uint32_t(uint16_t(rb)) << 16);
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const bool left = (bl[q] >> lane) & 1u, right = (br[q] >> lane) & 1u;
+        if (left || right) {
+          const int t = tq[q];
+          const uint32_t pk = pack[t];
+          const int np = left ? int(int16_t(pk & 0xffffu)) + int(bef[q] & 0xffffu)
+                              : int(int16_t(pk >> 16)) + int(bef[q] >> 16);
+          if (unsigned(np) < unsigned(TILE)) {
+            S.list[cur ^ 1][d][np] = eq[q];
+            if (d == 0) S.segOf[cur ^ 1][np] = uint16_t(2 * t + (right ? 1 : 0));
+          }
+        }
+      }
+      if (d + 1 < D) count_sides(d + 1);
     }
     __syncthreads();
-    // C: stable partition of every list (pivots dropped)
-    constexpr int PER = TILE / NT;
-    for (int d = 0; d < D; d++) {
-      const uint16_t *Lc = S.list[cur][d];
-      uint32_t local = 0;
-      const int p0 = tid * PER;
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const int p = p0 + q;
-        if (p < mact) {
-          const int f = S.flag[Lc[p]];
-          local += f == 0 ? 1u : (f == 1 ? 0x10000u : 0u);
-        }
-      }
-      uint32_t incl = local;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      if (lane == 31) S.warpSums[wid] = incl;
-      __syncthreads();
-      uint32_t wbase = 0;
-      for (int w = 0; w < wid; w++) wbase += S.warpSums[w];
-      uint32_t run = wbase + incl - local;
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const int p = p0 + q;
-        if (p < mact) {
-          S.scan[p] = run;
-          const int f = S.flag[Lc[p]];
-          run += f == 0 ? 1u : (f == 1 ? 0x10000u : 0u);
-        }
-      }
-      __syncthreads();
-      for (int p = tid; p < mact; p += NT) {
-        const int e = Lc[p];
-        const int f = S.flag[e];
-        if (f == 2) continue;
-        const int t = S.segOf[cur][p];
-        const int bt = S.u_sub.b[t];
-        const uint32_t sbase = S.scan[bt], sp = S.scan[p];
-        const int nb = bt - t;
-        const int np = f == 0 ? nb + int((sp & 0xffffu) - (sbase & 0xffffu))
-                              : nb + S.u_sub.r[t] + int((sp >> 16) - (sbase >> 16));
-        S.list[cur ^ 1][d][np] = uint16_t(e);
-        if (d == 0) S.segOf[cur ^ 1][np] = uint16_t(2 * t + f);
-      }
-      __syncthreads();
-    }
     mact -= nexist;
     cur ^= 1;
   }
@@ -1060,13 +1121,16 @@ __global__ void __launch_bounds__(kSubThreadsTree, 2) subtree_kernel(Bufs b, int
 // first) is exhausted.  A tree whose top-down phase ran L0 levels left its
 // records in key buffer L0 & 1.  Round-robin split dims.
 // threads per CTA of a tile class: 512 for 2048-point subtrees (as the single
-// tree's), 256 below (more resident CTAs; measured faster for those classes)
+// tree's), 256 below (more resident CTAs; measured faster for those classes);
+// the 256-thread classes are held to 64 registers, 4 CTAs per SM (measured
+// faster than the 72-96 registers the compiler picks unbounded)
 template <int TILE> struct ForestNT {
   static constexpr int value = TILE == 2048 ? kSubThreadsTree : kSubThreads;
+  static constexpr int minBlocks = TILE == 2048 ? 2 : 4;
 };
 
 template <int D, int TILE>
-__global__ void __launch_bounds__(ForestNT<TILE>::value, (ForestNT<TILE>::value > 256 ? 2 : 1))
+__global__ void __launch_bounds__(ForestNT<TILE>::value, ForestNT<TILE>::minBlocks)
     subtree_forest_kernel(Bufs b, ForestSubtrees f)
 {
   constexpr int NT = ForestNT<TILE>::value;
