@@ -1,10 +1,17 @@
 // kNN with host-resident queries and results: the queries are cut into
 // chunks that flow through three streams -- host->device copy, search
-// (cukd_knn on the caller's stream), device->host copy -- with two device
-// buffers per kind, so that copies of one chunk overlap the search of the
-// next.  For callers whose queries and answers live in host memory (the
-// reference's samples copy whole arrays with cudaMemcpy around one query
-// launch, sample.cu:121-160); results are those of cukd_knn.
+// (cukd_knn on the caller's stream), device->host copy -- with three device
+// buffer sets, so that the copies of one chunk overlap the searches of the
+// next ones.  A query buffer is reused once its search has run, a result
+// buffer once its answers are copied down, so the uploads stay off the path
+// of the result copies (the slowest stage when k is large: 128 bytes per
+// query at k = 16 against 12 up).  Measured on the 10M-query, k = 16
+// workload: 2^21-query chunks 27.8 ms, against 29.3 ms with two buffer sets;
+// chunk sizes ramping up from chunk/16 or /4, and a second search stream
+// taking every other chunk, measured 28-32 ms.  For callers whose queries
+// and answers live in host memory (the reference's samples copy whole
+// arrays with cudaMemcpy around one query launch, sample.cu:121-160);
+// results are those of cukd_knn.
 #include <algorithm>
 
 #include "common.cuh"
@@ -17,15 +24,41 @@ extern "C" int cukd_knn(const void *d_tree, int64_t n, const cukd_layout *layout
 namespace ckb {
 namespace {
 
+constexpr int kSets = 3;  // device buffer sets (queries, ids, d2)
+
 struct PipeRes {
   cudaStream_t up = nullptr, down = nullptr;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t upDone[kSets] = {}, searchDone[kSets] = {}, downDone[kSets] = {};
+  cudaEvent_t start = nullptr, join[2] = {};
   ~PipeRes()
   {
-    for (cudaEvent_t &e : ev)
+    for (int i = 0; i < kSets; i++) {
+      if (upDone[i]) cudaEventDestroy(upDone[i]);
+      if (searchDone[i]) cudaEventDestroy(searchDone[i]);
+      if (downDone[i]) cudaEventDestroy(downDone[i]);
+    }
+    if (start) cudaEventDestroy(start);
+    for (cudaEvent_t e : join)
       if (e) cudaEventDestroy(e);
     if (up) cudaStreamDestroy(up);
     if (down) cudaStreamDestroy(down);
+  }
+};
+
+// On every exit, success or error: the caller's stream waits for all work
+// queued on the side streams, so that the buffers released on it afterwards
+// (stream-ordered) are no longer in use.
+struct JoinSideStreams {
+  PipeRes &r;
+  cudaStream_t stream;
+  ~JoinSideStreams()
+  {
+    cudaStream_t side[2] = {r.up, r.down};
+    for (int i = 0; i < 2; i++) {
+      if (!side[i] || !r.join[i]) continue;
+      if (cudaEventRecord(r.join[i], side[i]) == cudaSuccess)
+        cudaStreamWaitEvent(stream, r.join[i], 0);
+    }
   }
 };
 
@@ -56,46 +89,53 @@ extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *l
     set_cuda_error(cudaGetLastError());
     return CUKD_ERR_CUDA;
   }
-  for (cudaEvent_t &e : r.ev)
-    CKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  cudaEvent_t *upDone = r.ev, *searchDone = r.ev + 2, *downDone = r.ev + 4, *start = r.ev + 6;
-  // buffers: [2] queries, ids, d2
+  for (int i = 0; i < kSets; i++) {
+    CKB_CUDA(cudaEventCreateWithFlags(&r.upDone[i], cudaEventDisableTiming));
+    CKB_CUDA(cudaEventCreateWithFlags(&r.searchDone[i], cudaEventDisableTiming));
+    CKB_CUDA(cudaEventCreateWithFlags(&r.downDone[i], cudaEventDisableTiming));
+  }
+  CKB_CUDA(cudaEventCreateWithFlags(&r.start, cudaEventDisableTiming));
+  for (cudaEvent_t &e : r.join) CKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+
   TempArena arena(stream, mem);
-  uint8_t *dq[2];
-  int32_t *di[2];
-  uint8_t *dd[2] = {nullptr, nullptr};
-  for (int b = 0; b < 2; b++) {
+  uint8_t *dq[kSets];
+  int32_t *di[kSets];
+  uint8_t *dd[kSets] = {};
+  for (int b = 0; b < kSets; b++) {
     CKB_TRY(arena.alloc(&dq[b], size_t(chunk * qBytes)));
     CKB_TRY(arena.alloc(&di[b], size_t(chunk * k)));
     if (h_out_d2) CKB_TRY(arena.alloc(&dd[b], size_t(chunk * k * d2Bytes)));
   }
+  // declared after the arena: joins the side streams before it releases
+  JoinSideStreams joiner{r, stream};
   // the side streams start after the work already queued on `stream`
-  CKB_CUDA(cudaEventRecord(start[0], stream));
-  CKB_CUDA(cudaStreamWaitEvent(r.up, start[0], 0));
-  CKB_CUDA(cudaStreamWaitEvent(r.down, start[0], 0));
+  CKB_CUDA(cudaEventRecord(r.start, stream));
+  CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
+  CKB_CUDA(cudaStreamWaitEvent(r.down, r.start, 0));
   const int64_t chunks = div_up(nq, chunk);
   for (int64_t c = 0; c < chunks; c++) {
-    const int b = int(c & 1);
+    const int b = int(c % kSets);
     const int64_t q0 = c * chunk, m = std::min(chunk, nq - q0);
-    if (c >= 2) CKB_CUDA(cudaStreamWaitEvent(r.up, downDone[b], 0));  // buffer b drained
+    // query buffer b: free once the search of chunk c - kSets has run
+    if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(r.up, r.searchDone[b], 0));
     CKB_CUDA(cudaMemcpyAsync(dq[b], (const uint8_t *)h_queries + q0 * qBytes, size_t(m * qBytes),
                              cudaMemcpyHostToDevice, r.up));
-    CKB_CUDA(cudaEventRecord(upDone[b], r.up));
-    CKB_CUDA(cudaStreamWaitEvent(stream, upDone[b], 0));
+    CKB_CUDA(cudaEventRecord(r.upDone[b], r.up));
+    CKB_CUDA(cudaStreamWaitEvent(stream, r.upDone[b], 0));
+    // result buffers b: free once chunk c - kSets' answers are copied down
+    if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(stream, r.downDone[b], 0));
     CKB_TRY(cukd_knn(d_tree, n, layout, d_world_bounds, dq[b], m, params, di[b], dd[b], nullptr,
                      stream, mem));
-    CKB_CUDA(cudaEventRecord(searchDone[b], stream));
-    CKB_CUDA(cudaStreamWaitEvent(r.down, searchDone[b], 0));
+    CKB_CUDA(cudaEventRecord(r.searchDone[b], stream));
+    CKB_CUDA(cudaStreamWaitEvent(r.down, r.searchDone[b], 0));
     CKB_CUDA(cudaMemcpyAsync(h_out_ids + q0 * k, di[b], size_t(m * k * 4), cudaMemcpyDeviceToHost,
                              r.down));
     if (h_out_d2)
       CKB_CUDA(cudaMemcpyAsync((uint8_t *)h_out_d2 + q0 * k * d2Bytes, dd[b],
                                size_t(m * k * d2Bytes), cudaMemcpyDeviceToHost, r.down));
-    CKB_CUDA(cudaEventRecord(downDone[b], r.down));
+    CKB_CUDA(cudaEventRecord(r.downDone[b], r.down));
   }
-  // the caller's stream completes after the last copy (and the buffers are
-  // released behind it)
-  CKB_CUDA(cudaEventRecord(start[1], r.down));
-  CKB_CUDA(cudaStreamWaitEvent(stream, start[1], 0));
+  // the caller's stream completes after the last copy (the joiner), and the
+  // buffers are released behind it
   return CUKD_OK;
 }

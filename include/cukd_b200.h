@@ -225,7 +225,8 @@ CUKD_API int cukd_knn(const void *d_tree, int64_t n, const cukd_layout *layout,
 
 /* cukd_knn with the queries and results in host memory: the queries are
  * processed in chunks of `chunk` (0 = 2^20) whose host->device copies,
- * searches and device->host copies overlap on three streams.  Results are
+ * searches and device->host copies overlap on three streams; device
+ * memory: three sets of chunk-sized query and result buffers.  Results are
  * cukd_knn's.  Use page-locked host buffers (cudaHostAlloc) for the copies
  * to overlap.  Returns once the work is queued; `stream` completes after the
  * last result copy.  No reference counterpart as one call (the reference's
