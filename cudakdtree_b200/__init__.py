@@ -28,8 +28,8 @@ import torch
 
 __all__ = [
     "lib", "Layout", "layout_for", "build_tree", "compute_bounds", "fcp", "knn",
-    "knn_visits", "morton_order", "CukdError", "STACK_BASED", "STACK_FREE", "CCT",
-    "BatchPlan",
+    "knn_visits", "knn_host", "knn_to_host", "morton_order", "CukdError", "STACK_BASED",
+    "STACK_FREE", "CCT", "BatchPlan",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -200,6 +200,8 @@ def lib():
         L.cukd_batch_autotune.argtypes = [C.c_void_p, P, P, C.c_int, C.POINTER(BatchTuning), P]
         L.cukd_knn_host.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
                                     C.POINTER(QueryParams), P, P, I64, P, P]
+        L.cukd_knn_to_host.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
+                                       C.POINTER(QueryParams), P, P, I64, P, P]
         L.cukd_knn_accumulate.argtypes = [P, I64, C.POINTER(Layout), P, I64, P, I64, P, C.c_int,
                                           C.c_float, C.c_int, P, P]
         L.cukd_knn_lists_extract.argtypes = [P, I64, C.c_int, P, P, P, P]
@@ -365,6 +367,34 @@ def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=N
     _check(lib().cukd_knn_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds), _ptr(queries),
                                nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk), _stream(stream),
                                None), "cukd_knn_host")
+    return ids, d2
+
+
+def knn_to_host(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
+                cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, out_ids=None, out_d2=None,
+                chunk=0, stream=None):
+    """knn() of device-resident queries with the answers written to host
+    memory (pinned CPU tensors by default), searches of query slices
+    overlapping the copies of earlier answers.  Returns (ids, d2) CPU
+    tensors, complete once ``stream`` (default: the current stream) is
+    synchronised."""
+    layout = layout or infer_layout(tree)
+    if n is None:
+        n = _num_records(tree, layout)
+    if not queries.is_cuda:
+        raise ValueError("queries must be device memory (use knn_host() for host queries)")
+    nq = queries.shape[0]
+    queries = queries.contiguous()
+    dt = torch.float32 if layout.scalar_type == FLOAT32 else torch.int64
+    ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32,
+                                                          pin_memory=True)
+    d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, pin_memory=True)
+    if ids.is_cuda or d2.is_cuda:
+        raise ValueError("out_ids / out_d2 must be host memory")
+    p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
+    _check(lib().cukd_knn_to_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                                  _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk),
+                                  _stream(stream), None), "cukd_knn_to_host")
     return ids, d2
 
 

@@ -1,17 +1,20 @@
-// kNN with host-resident queries and results: the queries are cut into
-// chunks that flow through three streams -- host->device copy, search
-// (cukd_knn on the caller's stream), device->host copy -- with three device
-// buffer sets, so that the copies of one chunk overlap the searches of the
-// next ones.  A query buffer is reused once its search has run, a result
-// buffer once its answers are copied down, so the uploads stay off the path
-// of the result copies (the slowest stage when k is large: 128 bytes per
-// query at k = 16 against 12 up).  Measured on the 10M-query, k = 16
-// workload: 2^21-query chunks 27.8 ms, against 29.3 ms with two buffer sets;
-// chunk sizes ramping up from chunk/16 or /4, and a second search stream
-// taking every other chunk, measured 28-32 ms.  For callers whose queries
-// and answers live in host memory (the reference's samples copy whole
-// arrays with cudaMemcpy around one query launch, sample.cu:121-160);
-// results are those of cukd_knn.
+// kNN whose answers go to host memory, in chunks that overlap the search of
+// one chunk with the device->host copy of the previous ones:
+//   cukd_knn_host     host-resident queries, uploaded chunk by chunk on a
+//                     side stream (three streams: up, search on the caller's
+//                     stream, down);
+//   cukd_knn_to_host  device-resident queries (the caller uploads them, e.g.
+//                     while the tree builds), two streams.
+// Three device buffer sets: a query buffer is reused once its search has
+// run, a result buffer once its answers are copied down, so the uploads stay
+// off the path of the result copies (the slowest stage when k is large: 128
+// bytes per query at k = 16 against 12 up).  Measured on the 10M-query,
+// k = 16 workload: 2^21-query chunks 27.8 ms, against 29.3 ms with two
+// buffer sets; chunk sizes ramping up from chunk/16 or /4, and a second
+// search stream taking every other chunk, measured 28-32 ms.  For callers
+// whose queries and answers live in host memory (the reference's samples
+// copy whole arrays with cudaMemcpy around one query launch,
+// sample.cu:121-160); results are those of cukd_knn.
 #include <algorithm>
 
 #include "common.cuh"
@@ -65,18 +68,23 @@ struct JoinSideStreams {
 }  // namespace
 }  // namespace ckb
 
-extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *layout,
-                             const void *d_world_bounds, const void *h_queries, int64_t nq,
-                             const cukd_query_params *params, int32_t *h_out_ids,
-                             void *h_out_d2, int64_t chunk, cudaStream_t stream,
-                             const cukd_mem_resource *mem)
+namespace ckb {
+namespace {
+
+// The chunked pipeline behind cukd_knn_host (h_queries set: chunks are
+// uploaded on a side stream) and cukd_knn_to_host (d_queries set: the
+// chunks are read in place).
+int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
+                 const void *d_world_bounds, const void *h_queries, const void *d_queries,
+                 int64_t nq, const cukd_query_params *params, int32_t *h_out_ids, void *h_out_d2,
+                 int64_t chunk, cudaStream_t stream, const cukd_mem_resource *mem)
 {
-  using namespace ckb;
   Layout L;
   if (!make_layout(layout, &L) || !params) return CUKD_ERR_INVALID_ARGUMENT;
   if (nq < 0 || params->k < 1 || params->k > 1024) return CUKD_ERR_INVALID_ARGUMENT;
   if (nq == 0) return CUKD_OK;
-  if (!h_queries || !h_out_ids) return CUKD_ERR_INVALID_ARGUMENT;
+  if ((!h_queries && !d_queries) || !h_out_ids) return CUKD_ERR_INVALID_ARGUMENT;
+  const bool upload = d_queries == nullptr;
   const int k = params->k;
   const int64_t qBytes = int64_t(L.D) * 4;
   const int64_t d2Bytes = L.scalar == CUKD_FLOAT32 ? 4 : 8;
@@ -84,7 +92,7 @@ extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *l
   chunk = std::min(chunk, nq);
 
   PipeRes r;
-  if (cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking) != cudaSuccess ||
+  if ((upload && cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking) != cudaSuccess) ||
       cudaStreamCreateWithFlags(&r.down, cudaStreamNonBlocking) != cudaSuccess) {
     set_cuda_error(cudaGetLastError());
     return CUKD_ERR_CUDA;
@@ -98,11 +106,11 @@ extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *l
   for (cudaEvent_t &e : r.join) CKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
   TempArena arena(stream, mem);
-  uint8_t *dq[kSets];
+  uint8_t *dq[kSets] = {};
   int32_t *di[kSets];
   uint8_t *dd[kSets] = {};
   for (int b = 0; b < kSets; b++) {
-    CKB_TRY(arena.alloc(&dq[b], size_t(chunk * qBytes)));
+    if (upload) CKB_TRY(arena.alloc(&dq[b], size_t(chunk * qBytes)));
     CKB_TRY(arena.alloc(&di[b], size_t(chunk * k)));
     if (h_out_d2) CKB_TRY(arena.alloc(&dd[b], size_t(chunk * k * d2Bytes)));
   }
@@ -110,21 +118,25 @@ extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *l
   JoinSideStreams joiner{r, stream};
   // the side streams start after the work already queued on `stream`
   CKB_CUDA(cudaEventRecord(r.start, stream));
-  CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
+  if (upload) CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
   CKB_CUDA(cudaStreamWaitEvent(r.down, r.start, 0));
   const int64_t chunks = div_up(nq, chunk);
   for (int64_t c = 0; c < chunks; c++) {
     const int b = int(c % kSets);
     const int64_t q0 = c * chunk, m = std::min(chunk, nq - q0);
-    // query buffer b: free once the search of chunk c - kSets has run
-    if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(r.up, r.searchDone[b], 0));
-    CKB_CUDA(cudaMemcpyAsync(dq[b], (const uint8_t *)h_queries + q0 * qBytes, size_t(m * qBytes),
-                             cudaMemcpyHostToDevice, r.up));
-    CKB_CUDA(cudaEventRecord(r.upDone[b], r.up));
-    CKB_CUDA(cudaStreamWaitEvent(stream, r.upDone[b], 0));
+    const void *qs = (const uint8_t *)d_queries + q0 * qBytes;
+    if (upload) {
+      // query buffer b: free once the search of chunk c - kSets has run
+      if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(r.up, r.searchDone[b], 0));
+      CKB_CUDA(cudaMemcpyAsync(dq[b], (const uint8_t *)h_queries + q0 * qBytes,
+                               size_t(m * qBytes), cudaMemcpyHostToDevice, r.up));
+      CKB_CUDA(cudaEventRecord(r.upDone[b], r.up));
+      CKB_CUDA(cudaStreamWaitEvent(stream, r.upDone[b], 0));
+      qs = dq[b];
+    }
     // result buffers b: free once chunk c - kSets' answers are copied down
     if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(stream, r.downDone[b], 0));
-    CKB_TRY(cukd_knn(d_tree, n, layout, d_world_bounds, dq[b], m, params, di[b], dd[b], nullptr,
+    CKB_TRY(cukd_knn(d_tree, n, layout, d_world_bounds, qs, m, params, di[b], dd[b], nullptr,
                      stream, mem));
     CKB_CUDA(cudaEventRecord(r.searchDone[b], stream));
     CKB_CUDA(cudaStreamWaitEvent(r.down, r.searchDone[b], 0));
@@ -138,4 +150,29 @@ extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *l
   // the caller's stream completes after the last copy (the joiner), and the
   // buffers are released behind it
   return CUKD_OK;
+}
+
+}  // namespace
+}  // namespace ckb
+
+extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *layout,
+                             const void *d_world_bounds, const void *h_queries, int64_t nq,
+                             const cukd_query_params *params, int32_t *h_out_ids,
+                             void *h_out_d2, int64_t chunk, cudaStream_t stream,
+                             const cukd_mem_resource *mem)
+{
+  if (nq > 0 && !h_queries) return CUKD_ERR_INVALID_ARGUMENT;
+  return ckb::knn_pipeline(d_tree, n, layout, d_world_bounds, h_queries, nullptr, nq, params,
+                           h_out_ids, h_out_d2, chunk, stream, mem);
+}
+
+extern "C" int cukd_knn_to_host(const void *d_tree, int64_t n, const cukd_layout *layout,
+                                const void *d_world_bounds, const void *d_queries, int64_t nq,
+                                const cukd_query_params *params, int32_t *h_out_ids,
+                                void *h_out_d2, int64_t chunk, cudaStream_t stream,
+                                const cukd_mem_resource *mem)
+{
+  if (nq > 0 && !d_queries) return CUKD_ERR_INVALID_ARGUMENT;
+  return ckb::knn_pipeline(d_tree, n, layout, d_world_bounds, nullptr, d_queries, nq, params,
+                           h_out_ids, h_out_d2, chunk, stream, mem);
 }

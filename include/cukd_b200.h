@@ -236,6 +236,19 @@ CUKD_API int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *lay
                            const cukd_query_params *params, int32_t *h_out_ids, void *h_out_d2,
                            int64_t chunk, cudaStream_t stream, const cukd_mem_resource *mem);
 
+/* cukd_knn_host for queries already in device memory: the searches of
+ * `chunk`-query slices of d_queries overlap the device->host copies of the
+ * answers of the previous slices (two streams; three sets of chunk-sized
+ * result buffers).  For callers that upload the queries themselves, e.g. on
+ * their own stream while the tree builds.  Results are cukd_knn's; `stream`
+ * completes after the last result copy.  No reference counterpart as one
+ * call (see cukd_knn_host). */
+CUKD_API int cukd_knn_to_host(const void *d_tree, int64_t n, const cukd_layout *layout,
+                              const void *d_world_bounds, const void *d_queries, int64_t nq,
+                              const cukd_query_params *params, int32_t *h_out_ids,
+                              void *h_out_d2, int64_t chunk, cudaStream_t stream,
+                              const cukd_mem_resource *mem);
+
 /* Per-query visited-node counts of the same traversal (the reference's
  * CUKD_ENABLE_STATS counter, cukd/common.h:345-360, per query). */
 CUKD_API int cukd_knn_visits(const void *d_tree, int64_t n, const cukd_layout *layout,

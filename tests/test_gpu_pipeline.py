@@ -1,7 +1,7 @@
-"""cukd_knn_host: kNN with host-resident queries and results, chunked over
-three overlapping streams -- its answers must equal cukd_knn's bit for bit,
-for pinned and pageable host memory and chunk sizes that do and do not
-divide the query count."""
+"""cukd_knn_host / cukd_knn_to_host: kNN with host-resident results (and
+host- or device-resident queries), chunked over overlapping streams -- their
+answers must equal cukd_knn's bit for bit, for pinned and pageable host
+memory and chunk sizes that do and do not divide the query count."""
 import numpy as np
 import pytest
 import torch
@@ -41,3 +41,32 @@ def test_knn_host_rejects_device_queries():
     t = torch.from_numpy(make_points(100, 3, "uniform", seed=1)).cuda()
     with pytest.raises(ValueError):
         ck.knn_host(t, t[:4], 4)
+
+
+@pytest.mark.parametrize("scalar", ["float32", "int32"])
+@pytest.mark.parametrize("k", [8, 40])
+@pytest.mark.parametrize("chunk", [0, 1000, 7777, 50000])
+def test_knn_to_host_equals_knn(scalar, k, chunk):
+    n, nq = 30000, 23456
+    pts = make_points(n, 3, "uniform", scalar=scalar, seed=5)
+    q = make_queries(nq, 3, "uniform", scalar=scalar, seed=6)
+    t = torch.from_numpy(pts).cuda()
+    lay = ck.layout_for(scalar, 3)
+    wb = ck.build_tree(t, layout=lay)
+    dq = torch.from_numpy(q).cuda()
+    ri, rd = ck.knn(t, dq, k, "stack_free", layout=lay, world_bounds=wb)
+    for _ in range(2):  # twice: buffers and streams of the first call are gone
+        ids, d2 = ck.knn_to_host(t, dq, k, "stack_free", layout=lay, world_bounds=wb, chunk=chunk)
+        torch.cuda.synchronize()
+        assert not ids.is_cuda and ids.is_pinned()
+        assert np.array_equal(ids.numpy(), ri.cpu().numpy())
+        if scalar == "float32":
+            assert np.array_equal(f32_bits(d2.numpy()), f32_bits(rd.cpu().numpy()))
+        else:
+            assert np.array_equal(d2.numpy(), rd.cpu().numpy())
+
+
+def test_knn_to_host_rejects_host_queries():
+    t = torch.from_numpy(make_points(100, 3, "uniform", seed=1)).cuda()
+    with pytest.raises(ValueError):
+        ck.knn_to_host(t, t[:4].cpu(), 4)
