@@ -132,16 +132,6 @@ struct HostLists {
   int64_t maxItems = 0, histCap = 0;
 };
 
-constexpr int kChunk = 4096;      // points per CTA of the level kernels (build.cu)
-constexpr int kMaxBins = 4096;
-
-static int pow2ceil(int64_t v)
-{
-  int p = 1;
-  while (p < v && p < (1 << 30)) p <<= 1;
-  return p;
-}
-
 // work lists of a forest whose subtree phase takes subtrees of <= tile points
 static void derive_lists(const std::vector<int64_t> &off, int tile, HostLists &h)
 {
@@ -187,8 +177,8 @@ static void derive_lists(const std::vector<int64_t> &off, int tile, HostLists &h
         vh.push_back(G[c] > l + 1 ? int32_t(nextFirst[c] + 2 * j) : -1);
       }
     }
-    h.nb[l] = std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / 512)));
-    h.cps[l] = int(div_up(std::max<int64_t>(maxSeg, 1), kChunk));
+    h.nb[l] = level_bins(maxSeg);
+    h.cps[l] = int(div_up(std::max<int64_t>(maxSeg, 1), kLevelChunk));
     h.maxItems = std::max(h.maxItems, cnt);
     h.histCap = std::max(h.histCap, cnt * h.nb[l]);
   }

@@ -41,6 +41,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "async.cuh"
 #include "common.cuh"
 #include "forest.cuh"
 
@@ -82,9 +83,17 @@ constexpr int kTile = 2048;       // max subtree size finished in shared memory
 // whichever measured faster
 constexpr int kSubThreads = 256;
 constexpr int kSubThreadsTree = 512;
-constexpr int kChunk = 4096;      // points per CTA in hist / partition
+constexpr int kChunk = kLevelChunk;  // points per CTA in hist / partition
 constexpr int kGThreads = 256;
 constexpr int kMaxBins = 4096;
+// partition staging: elements per array (a chunk plus 16-byte alignment slack)
+constexpr int kStageSpan = kChunk + 8;
+constexpr uint32_t kWaitPolls = 1u << 22;  // bound of a bulk-copy barrier wait
+// bulk-copy barrier waits that gave up: never expected (the copies read
+// memory the build owns), but a wait that does not complete must end the
+// kernel rather than hang it; the tree of that build is then wrong, and
+// cukd_async_wait_timeouts() reports the count
+__device__ unsigned int g_wait_timeouts = 0;
 constexpr int kBinPoints = 32;  // target points per histogram bin (global levels)
 
 struct Bufs {
@@ -361,19 +370,30 @@ __device__ inline void merge_child_bounds(uint32_t (&lo)[2][D], uint32_t (&hi)[2
     }
 }
 
-// Each warp owns a contiguous run of kChunk / 8 points and walks it 32 at a
-// time; per class (left / right / pivot-bin candidate) a ballot ranks the
-// lanes, so every store instruction writes one contiguous run per class
-// (the order inside a child's segment is irrelevant to the algorithm).
+// The CTA's chunk of keys and indices is staged in shared memory by one bulk
+// copy per array (TMA engine, all in flight at once; the partition was
+// load-latency bound with per-thread loads).  Each warp owns a contiguous
+// run of kChunk / 8 points and walks it 32 at a time; per class (left /
+// right / pivot-bin candidate) a ballot ranks the lanes, so every store
+// instruction writes one contiguous run per class (the order inside a
+// child's segment is irrelevant to the algorithm).
+template <int D>
+constexpr size_t partition_smem()
+{
+  return size_t(D + 1) * kStageSpan * sizeof(uint32_t);
+}
+
 template <int SC, int D>
-__global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelArgs a)
+__global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs a)
 {
   constexpr int W = kGThreads / 32;
   constexpr int PER_WARP = kChunk / W;
   constexpr int ROUNDS = PER_WARP / 32;
   static_assert(ROUNDS <= 16, "2-bit class codes packed in one uint32");
+  extern __shared__ __align__(128) uint32_t stage[];  // [D + 1][kStageSpan]
   __shared__ uint32_t warpTot[W][3];
   __shared__ uint32_t warpBase[W][3];
+  __shared__ __align__(8) uint64_t bar;
   const int seg = blockIdx.x / a.chunksPerSeg;
   const int chunk = blockIdx.x % a.chunksPerSeg;
   const SegGeo sg = seg_geo(a, seg);
@@ -387,10 +407,32 @@ __global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelAr
   const Binner<SC> bin(b.sbmin[0][seg * D + dim], b.sbmax[0][seg * D + dim], a.nb);
   const uint32_t pb = b.sel[seg * 3 + 0];
   const int cb = a.cb, nbuf = cb ^ 1;
-  const uint32_t *__restrict__ kd = b.key[cb][dim] + sb;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const uint32_t ltMask = (1u << lane) - 1u;
   const int64_t w0 = c0 + int64_t(wid) * PER_WARP;
+
+  // stage [a0, a1): the chunk with its start rounded down and its end up to
+  // 16 bytes (at most 3 extra elements a side, inside the arrays: their
+  // allocations are rounded up to 256 bytes)
+  const int64_t e0 = sb + c0, e1 = sb + c1;
+  const int64_t a0 = e0 & ~int64_t(3), a1 = (e1 + 3) & ~int64_t(3);
+  const uint32_t bytes = uint32_t(a1 - a0) * uint32_t(sizeof(uint32_t));
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(&bar, bytes * uint32_t(D + 1));
+#pragma unroll
+    for (int d = 0; d < D; d++) bulk_copy_g2s(stage + d * kStageSpan, b.key[cb][d] + a0, bytes, &bar);
+    bulk_copy_g2s(stage + D * kStageSpan, b.idx[cb] + a0, bytes, &bar);
+  }
+  if (!mbar_wait_bounded(&bar, 0, kWaitPolls)) {
+    if (threadIdx.x == 0) atomicAdd(&g_wait_timeouts, 1u);
+    mbar_wait_bounded(&bar, 0, kWaitPolls);  // let copies in flight land first
+    return;
+  }
+  // chunk position i (c0 <= i < c1) is staged element i - c0 + so
+  const int so = int(e0 - a0);
+  const uint32_t *kd = stage + dim * kStageSpan + so;
 
   // pass 1: class 0 = left, 1 = right, 2 = candidate; per-warp counts
   uint32_t cls = 0;
@@ -400,7 +442,7 @@ __global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelAr
     const int64_t i = w0 + r * 32 + lane;
     uint32_t c = 3;
     if (i < c1) {
-      const uint32_t bb = uint32_t(bin(kd[i]));
+      const uint32_t bb = uint32_t(bin(kd[int(i - c0)]));
       c = bb < pb ? 0u : (bb > pb ? 1u : 2u);
     }
     cls |= (c & 3u) << (2 * r);
@@ -436,9 +478,9 @@ __global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelAr
       lo[s][d] = 0xffffffffu;
       hi[s][d] = 0u;
     }
-  // pass 2: coalesced reads (four rounds' loads issued together), one
-  // contiguous write run per class per round.  Class-indexed values are
-  // picked with selects so that nothing lands in local memory.
+  // pass 2: reads from the staged chunk, one contiguous write run per class
+  // per round.  Class-indexed values are picked with selects so that
+  // nothing lands in local memory.
   constexpr int RB = 4;
   static_assert(ROUNDS % RB == 0, "rounds in batches");
   for (int r0 = 0; r0 < ROUNDS; r0 += RB) {
@@ -449,8 +491,8 @@ __global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelAr
       const uint32_t c = (cls >> (2 * (r0 + u))) & 3u;
       if (c < 3u) {
 #pragma unroll
-        for (int d = 0; d < D; d++) kk[u][d] = b.key[cb][d][sb + i];
-        idv[u] = b.idx[cb][sb + i];
+        for (int d = 0; d < D; d++) kk[u][d] = stage[d * kStageSpan + so + int(i - c0)];
+        idv[u] = stage[D * kStageSpan + so + int(i - c0)];
       }
     }
 #pragma unroll
@@ -494,6 +536,18 @@ __global__ void __launch_bounds__(kGThreads, 4) partition_kernel(Bufs b, LevelAr
     }
   }
   merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
+}
+
+// the staging area exceeds the default 48 KB of dynamic shared memory for
+// D >= 2: opt in (once per build, or at forest plan creation, outside any
+// graph capture)
+template <int SC, int D>
+int partition_opt_in()
+{
+  CKB_CUDA(cudaFuncSetAttribute(partition_kernel<SC, D>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(partition_smem<D>())));
+  return CUKD_OK;
 }
 
 // MSD radix select on the composite key among a subtree's candidates, then
@@ -1186,14 +1240,6 @@ static int pow2ceil(int64_t v)
   while (p < v && p < (1 << 30)) p <<= 1;
   return p;
 }
-// histogram bins of a global level: about kBinPoints points per bin of the
-// largest subtree, 64..kMaxBins.  Fewer points per bin leave fewer pivot-bin
-// candidates for resolve_kernel's radix select (one CTA per subtree); 512
-// per bin measured 6.38 ms for the 10M-point build, 128 6.13 ms, 32 6.12 ms.
-inline int level_bins(int64_t maxSeg)
-{
-  return std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / kBinPoints)));
-}
 
 template <int SC, int D>
 int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st,
@@ -1247,6 +1293,7 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
   root_kernel<SC, D><<<1, 32, 0, st>>>(b, worldBounds, explicitDims);
   CKB_CHECK_LAUNCH();
 
+  if (G > 0) CKB_TRY((partition_opt_in<SC, D>()));
   int cb = 0;
   for (int lvl = 0; lvl < G; lvl++) {
     const int nseg = 1 << lvl;
@@ -1266,7 +1313,7 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
     CKB_CHECK_LAUNCH();
     select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
     CKB_CHECK_LAUNCH();
-    partition_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
     CKB_CHECK_LAUNCH();
     resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
     CKB_CHECK_LAUNCH();
@@ -1466,6 +1513,7 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
   }
   root_kernel<SC, D><<<1, 32, 0, st>>>(b, worldBounds, explicitDims);
   CKB_CHECK_LAUNCH();
+  if (G > 0) CKB_TRY((partition_opt_in<SC, D>()));
   int cb = 0;
   for (int lvl = 0; lvl < G; lvl++) {
     const int nseg = 1 << lvl;
@@ -1485,7 +1533,7 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
     CKB_CHECK_LAUNCH();
     select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
     CKB_CHECK_LAUNCH();
-    partition_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
     CKB_CHECK_LAUNCH();
     resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
     CKB_CHECK_LAUNCH();
@@ -1630,7 +1678,7 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
     CKB_CHECK_LAUNCH();
     select_kernel<<<unsigned(div_up(int64_t(L.items) * 32, 256)), 256, 0, st>>>(b, a);
     CKB_CHECK_LAUNCH();
-    partition_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+    partition_kernel<0, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
     CKB_CHECK_LAUNCH();
     resolve_kernel<0, D><<<unsigned(L.items), kGThreads, 0, st>>>(b, a, false);
     CKB_CHECK_LAUNCH();
@@ -1694,6 +1742,16 @@ int subtree_occupancy()
 
 }  // namespace build
 
+// histogram bins of a global level: about kBinPoints points per bin of the
+// largest subtree, 64..kMaxBins.  Fewer points per bin leave fewer pivot-bin
+// candidates for resolve_kernel's radix select (one CTA per subtree); 512
+// per bin measured 6.38 ms for the 10M-point build, 128 6.13 ms, 32 6.12 ms.
+int level_bins(int64_t maxSeg)
+{
+  using namespace build;
+  return std::min(kMaxBins, std::max(64, pow2ceil(maxSeg / kBinPoints)));
+}
+
 int forest_workspace_create(ForestBuild *f, int64_t maxItems, int64_t histCap)
 {
   using namespace build;
@@ -1706,7 +1764,8 @@ int forest_workspace_create(ForestBuild *f, int64_t maxItems, int64_t histCap)
   const int64_t items = std::max<int64_t>(maxItems, 1);
   auto get = [&](auto **out, size_t count) -> int {
     void *p = nullptr;
-    const size_t bytes = std::max<size_t>(16, count * sizeof(**out));
+    // rounded up to 256 bytes: bulk copies read whole 16-byte units
+    const size_t bytes = (std::max<size_t>(16, count * sizeof(**out)) + 255) & ~size_t(255);
     if (cudaMalloc(&p, bytes) != cudaSuccess) {
       cudaGetLastError();
       return CUKD_ERR_OUT_OF_MEMORY;
@@ -1720,6 +1779,7 @@ int forest_workspace_create(ForestBuild *f, int64_t maxItems, int64_t histCap)
     if (rc == CUKD_OK) rc = r;
   };
   Bufs &b = ws->b;
+  T(D == 2 ? partition_opt_in<0, 2>() : (D == 3 ? partition_opt_in<0, 3>() : partition_opt_in<0, 4>()));
   for (int x = 0; x < 2; x++) {
     for (int d = 0; d < D; d++) T(get(&b.key[x][d], n));
     T(get(&b.idx[x], n));
@@ -1896,5 +1956,12 @@ const char *cukd_status_string(int status)
 const char *cukd_last_cuda_error(void) { return ckb::last_cuda_error_string(); }
 
 unsigned long long cukd_launch_count(void) { return ckb::launch_count(); }
+
+int cukd_async_wait_timeouts(unsigned int *count)
+{
+  if (!count) return CUKD_ERR_INVALID_ARGUMENT;
+  CKB_CUDA(cudaMemcpyFromSymbol(count, ckb::build::g_wait_timeouts, sizeof(unsigned int)));
+  return CUKD_OK;
+}
 
 }  // extern "C"

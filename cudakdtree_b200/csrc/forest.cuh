@@ -28,6 +28,12 @@ struct ForestLevel {
   const int32_t *cloud, *local, *child;
 };
 
+// geometry of the global (top-down) levels, shared by the single-tree
+// builder and the forest plan: points per CTA of the level kernels, and the
+// histogram bins of a level whose largest subtree holds maxSeg points
+constexpr int kLevelChunk = 4096;
+int level_bins(int64_t maxSeg);
+
 constexpr int kForestMaxLevels = 32;
 constexpr int kForestTiles[3] = {512, 1024, 2048};
 

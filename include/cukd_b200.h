@@ -475,6 +475,12 @@ CUKD_API const char *cukd_last_cuda_error(void);
  * observability counter, like the reference's CUKD_ENABLE_STATS hook,
  * cukd/common.h:345-360) */
 CUKD_API unsigned long long cukd_launch_count(void);
+/* number of bounded waits on bulk-copy barriers (the builder's partition
+ * pass) that gave up on the current device since the library was loaded;
+ * 0 unless something is badly wrong -- a kernel ends instead of hanging,
+ * and the tree of that build is then invalid.  Synchronises the device.
+ * No reference counterpart. */
+CUKD_API int cukd_async_wait_timeouts(unsigned int *count);
 
 #ifdef __cplusplus
 }

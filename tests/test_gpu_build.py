@@ -182,3 +182,18 @@ def test_tree_validity(explicit):
         dims = np.array([int(np.floor(np.log2(i + 1))) % 3 for i in range(n)])
     inf = np.full(3, np.inf, np.float32)
     _check_rec(tree, dims, n, -inf, inf, 0)
+
+
+def test_partition_staging_waits_never_give_up():
+    """The partition pass stages each chunk with bulk copies and waits on a
+    barrier with a bounded poll count; after builds whose chunks start and
+    end at every 16-byte phase (sizes 4097..4100 and a 10^6-point build)
+    no wait has given up."""
+    import ctypes
+    for n in (4097, 4098, 4099, 4100, 1_000_000):
+        t = torch.from_numpy(make_points(n, 3, "gmm", seed=n)).cuda()
+        ck.build_tree(t)
+    torch.cuda.synchronize()
+    count = ctypes.c_uint(7)
+    assert ck.lib().cukd_async_wait_timeouts(ctypes.byref(count)) == 0
+    assert count.value == 0
