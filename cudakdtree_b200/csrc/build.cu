@@ -77,12 +77,15 @@ const char *last_cuda_error_string() { return cudaGetErrorString(g_last_cuda); }
 namespace build {
 
 constexpr int ilog2_floor(int x) { return x <= 1 ? 0 : 1 + ilog2_floor(x >> 1); }
-constexpr int kTile = 2048;       // max subtree size finished in shared memory
-// threads of a subtree CTA: 512 (two resident CTAs per SM, 64 registers) for
-// 2048-point subtrees, 256 for the forest's 512- and 1024-point tile classes,
-// whichever measured faster
+// Max subtree size a single tree's subtree phase finishes in shared memory:
+// 1024 points (54 KB, 4 CTAs of 256 threads per SM) measured faster than
+// 2048 (108 KB, 2 per SM; one global level fewer) -- 10M points 5.60 against
+// 5.71 ms.  The forest keeps three tile classes (kForestTiles).
+constexpr int kTile = 1024;
+// threads of a subtree CTA, every tile class (for 2048-point tiles 256
+// measured faster than 512 with the ballot partitions: batched build 15.0
+// against 15.5 ms)
 constexpr int kSubThreads = 256;
-constexpr int kSubThreadsTree = 512;
 constexpr int kChunk = kLevelChunk;  // points per CTA in hist / partition
 constexpr int kGThreads = 256;
 constexpr int kMaxBins = 4096;
@@ -1160,14 +1163,14 @@ __device__ void subtree_body(const Bufs &b, int64_t n, int L0, int64_t s, int64_
 }
 
 template <int SC, int D>
-__global__ void __launch_bounds__(kSubThreadsTree, 2) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
+__global__ void __launch_bounds__(kSubThreads, 4) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
                                                               bool explicitDims)
 {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  SubSmem<D, kTile, kSubThreadsTree> &S =
-      *reinterpret_cast<SubSmem<D, kTile, kSubThreadsTree> *>(smem_raw);
+  SubSmem<D, kTile, kSubThreads> &S =
+      *reinterpret_cast<SubSmem<D, kTile, kSubThreads> *>(smem_raw);
   const int seg = blockIdx.x;
-  subtree_body<SC, D, kTile, kSubThreadsTree>(b, n, L0, ((int64_t(1) << L0) - 1) + seg, 0, seg, cb, explicitDims,
+  subtree_body<SC, D, kTile, kSubThreads>(b, n, L0, ((int64_t(1) << L0) - 1) + seg, 0, seg, cb, explicitDims,
                              S);
 }
 
@@ -1175,12 +1178,12 @@ __global__ void __launch_bounds__(kSubThreadsTree, 2) subtree_kernel(Bufs b, int
 // work item from a global counter until the list (sorted by size, largest
 // first) is exhausted.  A tree whose top-down phase ran L0 levels left its
 // records in key buffer L0 & 1.  Round-robin split dims.
-// threads per CTA of a tile class: 512 for 2048-point subtrees (as the single
-// tree's), 256 below (more resident CTAs; measured faster for those classes);
-// the 256-thread classes are held to 64 registers, 4 CTAs per SM (measured
-// faster than the 72-96 registers the compiler picks unbounded)
+// threads per CTA of a tile class (256 for all) and resident CTAs the
+// register budget targets: 4 per SM (64 registers; measured faster than the
+// 72-96 the compiler picks unbounded) for 512- and 1024-point tiles, 2 for
+// 2048-point tiles, whose 108 KB of shared memory allow no more
 template <int TILE> struct ForestNT {
-  static constexpr int value = TILE == 2048 ? kSubThreadsTree : kSubThreads;
+  static constexpr int value = kSubThreads;
   static constexpr int minBlocks = TILE == 2048 ? 2 : 4;
 };
 
@@ -1324,10 +1327,10 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
     std::swap(b.sbox[0], b.sbox[1]);
   }
   {
-    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreadsTree>);
+    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreads>);
     CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreadsTree, smem, st>>>(b, n, G, cb,
+    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
                                                                        explicitDims);
     CKB_CHECK_LAUNCH();
   }
@@ -1544,10 +1547,10 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
     std::swap(b.sbox[0], b.sbox[1]);
   }
   {
-    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreadsTree>);
+    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreads>);
     CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreadsTree, smem, st>>>(b, n, G, cb,
+    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
                                                                        explicitDims);
     CKB_CHECK_LAUNCH();
   }

@@ -18,8 +18,8 @@ from tests.helpers import make_points
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [1, 2, 3, 4, 5, 7, 8, 10, 31, 100, 1000, 2047, 2048, 2049, 3000, 4097, 10000,
-         50000, 200000]
+SIZES = [1, 2, 3, 4, 5, 7, 8, 10, 31, 100, 1000, 1023, 1024, 1025, 2047, 2048, 2049, 3000,
+         4097, 10000, 50000, 200000]
 
 
 def _gpu_build_plain(pts, builder="default"):
@@ -60,7 +60,7 @@ def _payload_records(pts):
     return rec
 
 
-@pytest.mark.parametrize("n", [1, 2, 100, 2049, 20000, 100000])
+@pytest.mark.parametrize("n", [1, 2, 100, 1025, 2049, 20000, 100000])
 @pytest.mark.parametrize("kind", ["tie", "same", "gmm"])
 def test_payload_order_follows_input_index(n, kind):
     """Identical points must come out in the reference's order too: the
