@@ -249,7 +249,11 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   } else if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32) {
     int32_t *perm = nullptr;
     CKB_TRY(arena.alloc(&perm, nq));
-    CKB_TRY(morton_order_impl((const float *)d_queries, nq, L.D, nullptr, perm, st, mem));
+    // the Morton grid spans the tree's world bounds when the caller passes
+    // them (no bounds pass over the queries; queries outside are clamped to
+    // the box faces, which only coarsens their order), else the queries' own
+    CKB_TRY(morton_order_impl((const float *)d_queries, nq, L.D, (const float *)d_world_bounds,
+                              perm, st, mem));
     a.order = perm;
   }
   // fast exact path (see fast.cu): any visiting order, boundary-tie check,
