@@ -126,6 +126,7 @@ struct HostLists {
   std::vector<int32_t> lvCloud[kForestMaxLevels], lvLocal[kForestMaxLevels],
       lvChild[kForestMaxLevels];
   int nb[kForestMaxLevels], cps[kForestMaxLevels];
+  int64_t maxSeg[kForestMaxLevels];
   std::vector<int32_t> rootItem;
   std::vector<int32_t> subCloud[3], subLocal[3];
   std::vector<int8_t> subLevel[3];
@@ -179,6 +180,7 @@ static void derive_lists(const std::vector<int64_t> &off, int tile, HostLists &h
     }
     h.nb[l] = level_bins(maxSeg);
     h.cps[l] = int(div_up(std::max<int64_t>(maxSeg, 1), kLevelChunk));
+    h.maxSeg[l] = maxSeg;
     h.maxItems = std::max(h.maxItems, cnt);
     h.histCap = std::max(h.histCap, cnt * h.nb[l]);
   }
@@ -322,6 +324,7 @@ static int install_tile(cukd_batch_plan_s *p, int tile)
     L.items = int(h.lvCloud[l].size());
     L.nb = h.nb[l];
     L.chunksPerSeg = h.cps[l];
+    L.maxSeg = h.maxSeg[l];
     L.cloud = base + at[x++];
     L.local = base + at[x++];
     L.child = base + at[x++];

@@ -91,6 +91,9 @@ constexpr int kGThreads = 256;
 constexpr int kMaxBins = 4096;
 // partition staging: elements per array (a chunk plus 16-byte alignment slack)
 constexpr int kStageSpan = kChunk + 8;
+// global levels whose largest subtree holds at most this many points run
+// level_fused_kernel (10M-point build: 5.61 -> 5.43 ms)
+constexpr int64_t kFusedMax = kChunk;
 constexpr uint32_t kWaitPolls = 1u << 22;  // bound of a bulk-copy barrier wait
 // bulk-copy barrier waits that gave up: never expected (the copies read
 // memory the build owns), but a wait that does not complete must end the
@@ -541,18 +544,6 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
   merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
 }
 
-// the staging area exceeds the default 48 KB of dynamic shared memory for
-// D >= 2: opt in (once per build, or at forest plan creation, outside any
-// graph capture)
-template <int SC, int D>
-int partition_opt_in()
-{
-  CKB_CUDA(cudaFuncSetAttribute(partition_kernel<SC, D>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(partition_smem<D>())));
-  return CUKD_OK;
-}
-
 // MSD radix select on the composite key among a subtree's candidates, then
 // the candidates' final placement.  One CTA per subtree.
 template <int SC, int D>
@@ -735,6 +726,266 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
                                    : uint8_t((a.level + 1) % D);
     }
   }
+}
+
+// One whole global level for subtrees of at most kChunk points, one CTA per
+// subtree, in place of hist / select / partition / resolve (at the deepest
+// global levels those launches were bound by per-CTA latency, not by
+// bandwidth).  The subtree is staged in shared memory by bulk copies; the
+// point of rank leftSize(g) under the composite key is found by an MSD radix
+// select over the staged words (the split-dim key's digits taken over its
+// data span, so 2-3 passes instead of 4); the other points go to the
+// children's segments.  Same pivot, same children's sets and bounds as the
+// four-kernel path (the order inside a child's segment is irrelevant).
+template <int SC, int D>
+__global__ void __launch_bounds__(kGThreads) level_fused_kernel(Bufs b, LevelArgs a,
+                                                                bool explicitDims)
+{
+  extern __shared__ __align__(128) uint32_t stage[];  // [D + 1][kStageSpan]
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr;
+  __shared__ uint32_t pw[D + 1];
+  __shared__ __align__(8) uint64_t bar;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int seg = blockIdx.x;
+  const SegGeo sg = seg_geo(a, seg);
+  const int64_t g = sg.g;
+  const int64_t sb = sg.base + seg_begin(g, a.level, sg.n);
+  const int64_t sz = subtree_size(g, sg.n);
+  if (sz < 1 || sz > kChunk) return;  // the host launches this for sz <= kChunk only
+  const uint32_t m = uint32_t(sz);
+  const uint32_t r = uint32_t(left_size(g, sg.n));
+  const int dim = b.sdim[0][seg];
+
+  // composite order: own dim, then ancestors' dims nearest first, then index
+  int cd[D];
+  int ncd = 0;
+  cd[ncd++] = dim;
+  for (int64_t an = g; an > 0 && ncd < D;) {
+    an = (an - 1) >> 1;
+    const int da = explicitDims ? int(b.ndim[sg.base + an]) : rr_dim(an, D);
+    bool seen = false;
+    for (int i = 0; i < ncd; i++) seen |= (cd[i] == da);
+    if (!seen) cd[ncd++] = da;
+  }
+  const int nwords = ncd + 1;
+
+  // stage the subtree (16-byte-aligned span, as in partition_kernel)
+  const int64_t a0 = sb & ~int64_t(3), a1 = (sb + sz + 3) & ~int64_t(3);
+  const uint32_t bytes = uint32_t(a1 - a0) * uint32_t(sizeof(uint32_t));
+  const int cb = a.cb, nbuf = cb ^ 1;
+  if (tid == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar, bytes * uint32_t(D + 1));
+#pragma unroll
+    for (int d = 0; d < D; d++) bulk_copy_g2s(stage + d * kStageSpan, b.key[cb][d] + a0, bytes, &bar);
+    bulk_copy_g2s(stage + D * kStageSpan, b.idx[cb] + a0, bytes, &bar);
+  }
+  if (!mbar_wait_bounded(&bar, 0, kWaitPolls)) {
+    if (tid == 0) atomicAdd(&g_wait_timeouts, 1u);
+    mbar_wait_bounded(&bar, 0, kWaitPolls);  // let copies in flight land first
+    return;
+  }
+  const uint32_t *sw = stage + int(sb - a0);  // staged element i: sw[x * kStageSpan + i]
+  auto word = [&](uint32_t i, int w) -> uint32_t {
+    return sw[(w < ncd ? cd[w] : D) * kStageSpan + int(i)];
+  };
+
+  // MSD radix select of rank r
+  const uint32_t klo = b.sbmin[0][seg * D + dim], khi = b.sbmax[0][seg * D + dim];
+  uint32_t rank = r;
+  bool unique = false;
+  int w = 0;
+  uint32_t cp = 0, cm = 0, base = 0;
+  for (w = 0; w < nwords && !unique; w++) {
+    cp = 0;
+    cm = 0;
+    base = w == 0 ? klo : 0u;
+    const uint32_t span = w == 0 ? (khi >= klo ? khi - klo : 0u) : 0xffffffffu;
+    const int top = span ? ((31 - __clz(span)) & ~7) : -8;  // no digit: one value
+    for (int shift = top; shift >= 0; shift -= 8) {
+      for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+      __syncthreads();
+      for (uint32_t i = tid; i < m; i += blockDim.x) {
+        bool ok = true;
+        for (int q = 0; q < w && ok; q++) ok = word(i, q) == pw[q];
+        if (!ok) continue;
+        const uint32_t v = word(i, w) - base;
+        if ((v & cm) != cp) continue;
+        atomicAdd(&hist[(v >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (tid < 32) {
+        uint32_t s8 = 0;
+        for (int k = 0; k < 8; k++) s8 += hist[lane * 8 + k];
+        uint32_t incl = s8;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const uint32_t excl = incl - s8;
+        if (rank >= excl && rank < incl) {
+          uint32_t cum = excl;
+          for (int k = 0; k < 8; k++) {
+            const uint32_t c = hist[lane * 8 + k];
+            if (rank < cum + c) {
+              sDigit = uint32_t(lane * 8 + k);
+              sCount = c;
+              sRank = rank - cum;
+              break;
+            }
+            cum += c;
+          }
+        }
+      }
+      __syncthreads();
+      rank = sRank;
+      cp |= sDigit << shift;
+      cm |= 0xffu << shift;
+      if (sCount == 1) {
+        unique = true;
+        break;
+      }
+    }
+    if (!unique && tid == 0) pw[w] = cp + base;
+    __syncthreads();
+  }
+  // the word at which the pivot became unique (w ran one past it), else
+  // every word fully resolved
+  const int wl = unique ? w - 1 : nwords - 1;
+  if (!unique) {
+    cp = pw[nwords - 1];
+    cm = 0xffffffffu;
+    base = 0;
+  }
+  if (tid == 0) {
+    sPivot = 0xffffffffu;
+    sNl = 0;
+    sNr = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < m; i += blockDim.x) {
+    bool ok = true;
+    for (int q = 0; q < wl && ok; q++) ok = word(i, q) == pw[q];
+    if (ok && ((word(i, wl) - base) & cm) == cp) sPivot = i;
+  }
+  __syncthreads();
+  // exactly one point matches; the clamp only guards memory safety
+  const uint32_t piv = sPivot < m ? sPivot : 0u;
+  uint32_t pk[D + 1];
+#pragma unroll
+  for (int x = 0; x < D + 1; x++) pk[x] = x < nwords ? word(piv, x) : 0u;
+  uint32_t pkey[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) pkey[d] = sw[d * kStageSpan + int(piv)];
+
+  // the other points to the children, warp-contiguous runs per side
+  const int64_t lchild = 2 * g + 1;
+  const int lvlNext = a.level + 1;
+  const int64_t lBeg = sg.base + seg_begin(lchild, lvlNext, sg.n);
+  const int64_t rBeg = sg.base + seg_begin(lchild + 1, lvlNext, sg.n);
+  const uint32_t lsz = r, rsz = m - 1u - r;
+  const uint32_t ltMask = (1u << lane) - 1u;
+  uint32_t lo[2][D], hi[2][D];
+#pragma unroll
+  for (int s2 = 0; s2 < 2; s2++)
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      lo[s2][d] = 0xffffffffu;
+      hi[s2][d] = 0u;
+    }
+  for (uint32_t i0 = 0; i0 < m; i0 += blockDim.x) {
+    const uint32_t i = i0 + tid;
+    const bool valid = i < m && i != piv;
+    int side = 0;
+    if (valid) {
+      bool decided = false;
+#pragma unroll
+      for (int x = 0; x < D + 1; x++) {
+        if (x < nwords && !decided) {
+          const uint32_t v = word(i, x);
+          if (v != pk[x]) {
+            side = v > pk[x];
+            decided = true;
+          }
+        }
+      }
+    }
+    const uint32_t ml = __ballot_sync(0xffffffffu, valid && side == 0);
+    const uint32_t mr = __ballot_sync(0xffffffffu, valid && side == 1);
+    uint32_t bl = 0, br = 0;
+    if (lane == 0) {
+      if (ml) bl = atomicAdd(&sNl, uint32_t(__popc(ml)));
+      if (mr) br = atomicAdd(&sNr, uint32_t(__popc(mr)));
+    }
+    bl = __shfl_sync(0xffffffffu, bl, 0);
+    br = __shfl_sync(0xffffffffu, br, 0);
+    if (valid) {
+      const uint32_t pos = side ? br + __popc(mr & ltMask) : bl + __popc(ml & ltMask);
+      if (pos < (side ? rsz : lsz)) {
+        const int64_t dst = (side ? rBeg : lBeg) + pos;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const uint32_t k = sw[d * kStageSpan + int(i)];
+          b.key[nbuf][d][dst] = k;
+          if (side) {
+            lo[1][d] = min(lo[1][d], k);
+            hi[1][d] = max(hi[1][d], k);
+          } else {
+            lo[0][d] = min(lo[0][d], k);
+            hi[0][d] = max(hi[0][d], k);
+          }
+        }
+        b.idx[nbuf][dst] = sw[D * kStageSpan + int(i)];
+      }
+    }
+  }
+  merge_child_bounds<D>(lo, hi, b.sbmin[1], b.sbmax[1], sg.child);
+  if (tid == 0) {
+    b.perm[sg.base + g] = sw[D * kStageSpan + int(piv)];
+    b.ndim[sg.base + g] = uint8_t(dim);
+  }
+  if (tid == 0 && sg.child >= 0) {
+    uint32_t bl3[D], bh3[D];
+    for (int d = 0; d < D; d++) {
+      bl3[d] = b.sbox[0][int64_t(seg) * 2 * D + d];
+      bh3[d] = b.sbox[0][int64_t(seg) * 2 * D + D + d];
+    }
+    for (int s2 = 0; s2 < 2; s2++) {
+      uint32_t cl[D], ch[D];
+      for (int d = 0; d < D; d++) {
+        cl[d] = bl3[d];
+        ch[d] = bh3[d];
+      }
+      if (s2 == 0)
+        ch[dim] = pkey[dim];
+      else
+        cl[dim] = pkey[dim];
+      const int64_t ci = sg.child + s2;
+      for (int d = 0; d < D; d++) {
+        b.sbox[1][ci * 2 * D + d] = cl[d];
+        b.sbox[1][ci * 2 * D + D + d] = ch[d];
+      }
+      b.sdim[1][ci] = explicitDims ? uint8_t(Scalar<SC>::widest(cl, ch, D))
+                                   : uint8_t((a.level + 1) % D);
+    }
+  }
+}
+
+// the staging area exceeds the default 48 KB of dynamic shared memory for
+// D >= 2: opt in (once per build, or at forest plan creation, outside any
+// graph capture)
+template <int SC, int D>
+int partition_opt_in()
+{
+  CKB_CUDA(cudaFuncSetAttribute(partition_kernel<SC, D>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(partition_smem<D>())));
+  CKB_CUDA(cudaFuncSetAttribute(level_fused_kernel<SC, D>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(partition_smem<D>())));
+  return CUKD_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1308,18 +1559,23 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
     a.chunksPerSeg = int(div_up(maxSeg, kChunk));
     a.nseg = nseg;
     a.cb = cb;
-    CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
     CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * 2 * nseg * D, st));
     CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * 2 * nseg * D, st));
-    const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
-    hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
-    CKB_CHECK_LAUNCH();
+    if (maxSeg <= kFusedMax) {
+      level_fused_kernel<SC, D><<<nseg, kGThreads, partition_smem<D>(), st>>>(b, a, explicitDims);
+      CKB_CHECK_LAUNCH();
+    } else {
+      CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
+      const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
+      hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
+      CKB_CHECK_LAUNCH();
+    }
     cb ^= 1;
     std::swap(b.sdim[0], b.sdim[1]);
     std::swap(b.sbmin[0], b.sbmin[1]);
@@ -1528,18 +1784,23 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
     a.chunksPerSeg = int(div_up(maxSeg, kChunk));
     a.nseg = nseg;
     a.cb = cb;
-    CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
     CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * 2 * nseg * D, st));
     CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * 2 * nseg * D, st));
-    const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
-    hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
-    CKB_CHECK_LAUNCH();
+    if (maxSeg <= kFusedMax) {
+      level_fused_kernel<SC, D><<<nseg, kGThreads, partition_smem<D>(), st>>>(b, a, explicitDims);
+      CKB_CHECK_LAUNCH();
+    } else {
+      CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
+      const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
+      hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
+      CKB_CHECK_LAUNCH();
+    }
     cb ^= 1;
     std::swap(b.sdim[0], b.sdim[1]);
     std::swap(b.sbmin[0], b.sbmin[1]);
@@ -1671,20 +1932,26 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
     a.wChild = L.child;
     a.cBase = f.cloudBase;
     a.cN = f.cloudN;
-    CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(L.items) * L.nb, st));
     if (nextItems > 0) {
       CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * size_t(nextItems) * D, st));
       CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * size_t(nextItems) * D, st));
     }
-    const int64_t grid = int64_t(L.items) * L.chunksPerSeg;
-    hist_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    select_kernel<<<unsigned(div_up(int64_t(L.items) * 32, 256)), 256, 0, st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    partition_kernel<0, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
-    CKB_CHECK_LAUNCH();
-    resolve_kernel<0, D><<<unsigned(L.items), kGThreads, 0, st>>>(b, a, false);
-    CKB_CHECK_LAUNCH();
+    if (L.maxSeg <= kFusedMax) {
+      level_fused_kernel<0, D><<<unsigned(L.items), kGThreads, partition_smem<D>(), st>>>(b, a,
+                                                                                          false);
+      CKB_CHECK_LAUNCH();
+    } else {
+      CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(L.items) * L.nb, st));
+      const int64_t grid = int64_t(L.items) * L.chunksPerSeg;
+      hist_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      select_kernel<<<unsigned(div_up(int64_t(L.items) * 32, 256)), 256, 0, st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      partition_kernel<0, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
+      CKB_CHECK_LAUNCH();
+      resolve_kernel<0, D><<<unsigned(L.items), kGThreads, 0, st>>>(b, a, false);
+      CKB_CHECK_LAUNCH();
+    }
     cb ^= 1;
     std::swap(b.sdim[0], b.sdim[1]);
     std::swap(b.sbmin[0], b.sbmin[1]);

@@ -25,6 +25,7 @@ struct ForestSubtrees {
 // children go to the subtree phase)
 struct ForestLevel {
   int items, nb, chunksPerSeg;
+  int64_t maxSeg;  // points of the level's largest subtree
   const int32_t *cloud, *local, *child;
 };
 
