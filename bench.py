@@ -357,10 +357,31 @@ def run_ours(args, rank, world, local):
 
         et = timed(e2e_step)
         dt = timed(device_queries_step)
+
+        # the PCIe copies alone (one whole-array copy each way, pinned host
+        # memory): the floor under any e2e step that moves these bytes
+        def copy_ms(fn, reps=3):
+            best = None
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                fn()
+                b.record()
+                torch.cuda.synchronize()
+                best = a.elapsed_time(b) if best is None else min(best, a.elapsed_time(b))
+            return best
+        d_res = torch.empty((nq, K), dtype=torch.int32, device=dev)
+        d_tmp = torch.empty_like(d_pts)  # d_pts keeps the built tree
+        up_ms = copy_ms(lambda: (d_tmp.copy_(h_pts, non_blocking=True),
+                                 e2e_q.copy_(h_q, non_blocking=True)))
+        down_ms = copy_ms(lambda: (h_ids.copy_(d_res, non_blocking=True),
+                                   h_d2.view(torch.int32).copy_(d_res, non_blocking=True)))
+        del d_res, d_tmp
         e2e = {"value": round(whole_job_rate(nq, world, et), 1), "unit": UNIT,
                "h2d_bytes_per_step": int(h_pts.numel() * 4 + h_q.numel() * 4),
                "d2h_bytes_per_step": int(h_ids.numel() * 4 + h_d2.numel() * 4),
                "ms_per_step": round(et, 3),
+               "pcie_copies_alone_ms": {"h2d": round(up_ms, 3), "d2h": round(down_ms, 3)},
                "api": (f"cukd_build_tree + cukd_knn_host (pinned host queries and results, "
                        f"{args.e2e_chunk}-query chunks on overlapping copy / search streams)"),
                "device_queries_api": {
