@@ -360,7 +360,7 @@ def run_ours(args, rank, world, local):
 
         # the PCIe copies alone (one whole-array copy each way, pinned host
         # memory): the floor under any e2e step that moves these bytes
-        def copy_ms(fn, reps=3):
+        def pcie_ms(fn, reps=3):
             best = None
             for _ in range(reps):
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -372,9 +372,9 @@ def run_ours(args, rank, world, local):
             return best
         d_res = torch.empty((nq, K), dtype=torch.int32, device=dev)
         d_tmp = torch.empty_like(d_pts)  # d_pts keeps the built tree
-        up_ms = copy_ms(lambda: (d_tmp.copy_(h_pts, non_blocking=True),
+        up_ms = pcie_ms(lambda: (d_tmp.copy_(h_pts, non_blocking=True),
                                  e2e_q.copy_(h_q, non_blocking=True)))
-        down_ms = copy_ms(lambda: (h_ids.copy_(d_res, non_blocking=True),
+        down_ms = pcie_ms(lambda: (h_ids.copy_(d_res, non_blocking=True),
                                    h_d2.view(torch.int32).copy_(d_res, non_blocking=True)))
         del d_res, d_tmp
         e2e = {"value": round(whole_job_rate(nq, world, et), 1), "unit": UNIT,

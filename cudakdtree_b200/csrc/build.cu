@@ -14,7 +14,8 @@
 //  subtrees of a level are processed by the same launches:
 //    hist_kernel      histogram of the split coordinate into equal-width
 //                     bins over the subtree's data range
-//    select_kernel    the bin holding rank leftSize(g) (one warp/subtree)
+//    select_kernel    the bin holding rank leftSize(g) (a warp or a CTA per
+//                     subtree)
 //    partition_kernel points of lower bins -> left child's segment, higher
 //                     bins -> right child's segment, the pivot bin's points
 //                     -> candidate buffer; grows the children's data bounds
@@ -352,6 +353,45 @@ __global__ void select_kernel(Bufs b, LevelArgs a)
     }
   }
   if (lane < 3) b.cur[warp * 3 + lane] = 0;
+}
+
+// the same with one 256-thread CTA per subtree, for levels with >= 512 bins
+// (a warp summing 128 bins per lane was latency bound there)
+__global__ void __launch_bounds__(256) select_block_kernel(Bufs b, LevelArgs a)
+{
+  __shared__ uint32_t warpSum[8];
+  const int seg = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const SegGeo sg = seg_geo(a, seg);
+  const uint32_t r = uint32_t(left_size(sg.g, sg.n));
+  const uint32_t *h = b.hist + int64_t(seg) * a.nb;
+  const int per = a.nb / 256;
+  uint32_t s = 0;
+  for (int i = 0; i < per; i++) s += h[tid * per + i];
+  uint32_t incl = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warpSum[wid] = incl;
+  __syncthreads();
+  uint32_t wbase = 0;
+  for (int w = 0; w < wid; w++) wbase += warpSum[w];
+  const uint32_t excl = wbase + incl - s;
+  if (r >= excl && r < excl + s) {
+    uint32_t cum = excl;
+    for (int i = 0; i < per; i++) {
+      const uint32_t c = h[tid * per + i];
+      if (r < cum + c) {
+        b.sel[seg * 3 + 0] = uint32_t(tid * per + i);
+        b.sel[seg * 3 + 1] = cum;
+        b.sel[seg * 3 + 2] = c;
+        break;
+      }
+      cum += c;
+    }
+  }
+  if (tid < 3) b.cur[seg * 3 + tid] = 0;
 }
 
 // warp-reduce per-child bounds and merge them into the next level's arrays
@@ -1569,7 +1609,10 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
       const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
       hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
-      select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
+      if (a.nb >= 512)
+        select_block_kernel<<<unsigned(nseg), 256, 0, st>>>(b, a);
+      else
+        select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
       partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
       CKB_CHECK_LAUNCH();
@@ -1794,7 +1837,10 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
       const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
       hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
-      select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
+      if (a.nb >= 512)
+        select_block_kernel<<<unsigned(nseg), 256, 0, st>>>(b, a);
+      else
+        select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
       partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
       CKB_CHECK_LAUNCH();
@@ -1945,7 +1991,10 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
       const int64_t grid = int64_t(L.items) * L.chunksPerSeg;
       hist_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
-      select_kernel<<<unsigned(div_up(int64_t(L.items) * 32, 256)), 256, 0, st>>>(b, a);
+      if (a.nb >= 512)
+        select_block_kernel<<<unsigned(L.items), 256, 0, st>>>(b, a);
+      else
+        select_kernel<<<unsigned(div_up(int64_t(L.items) * 32, 256)), 256, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
       partition_kernel<0, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
       CKB_CHECK_LAUNCH();
