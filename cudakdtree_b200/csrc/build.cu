@@ -92,6 +92,10 @@ constexpr int kGThreads = 256;
 constexpr int kMaxBins = 4096;
 // partition staging: elements per array (a chunk plus 16-byte alignment slack)
 constexpr int kStageSpan = kChunk + 8;
+// partition chunks per hist_kernel CTA: fewer CTAs merge fewer bin counts
+// into the global histogram with atomics (10M-point build: 1 -> 5.27 ms,
+// 4 -> 5.14 ms, 8 -> 5.23 ms)
+constexpr int kHistGroup = 4;
 // global levels whose largest subtree holds at most this many points run
 // level_fused_kernel (10M-point build: 5.61 -> 5.43 ms)
 constexpr int64_t kFusedMax = kChunk;
@@ -301,14 +305,15 @@ template <int SC, int D>
 __global__ void __launch_bounds__(kGThreads) hist_kernel(Bufs b, LevelArgs a)
 {
   __shared__ uint32_t sh[kMaxBins];
-  const int seg = blockIdx.x / a.chunksPerSeg;
-  const int chunk = blockIdx.x % a.chunksPerSeg;
+  const int groups = (a.chunksPerSeg + kHistGroup - 1) / kHistGroup;
+  const int seg = blockIdx.x / groups;
+  const int grp = blockIdx.x % groups;
   const SegGeo sg = seg_geo(a, seg);
   const int64_t sb = sg.base + seg_begin(sg.g, a.level, sg.n);
   const int64_t sz = subtree_size(sg.g, sg.n);
-  const int64_t c0 = int64_t(chunk) * kChunk;
+  const int64_t c0 = int64_t(grp) * kHistGroup * kChunk;
   if (c0 >= sz) return;
-  const int64_t c1 = min(sz, c0 + kChunk);
+  const int64_t c1 = min(sz, c0 + int64_t(kHistGroup) * kChunk);
   for (int i = threadIdx.x; i < a.nb; i += blockDim.x) sh[i] = 0;
   __syncthreads();
   const int dim = b.sdim[0][seg];
@@ -591,9 +596,13 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
                                                             bool explicitDims)
 {
   __shared__ uint32_t hist[256];
-  __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr;
+  __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr, sLo, sHi;
   __shared__ uint32_t pw[D + 1];
   const int seg = blockIdx.x;
+  if (threadIdx.x == 0) {
+    sLo = 0xffffffffu;
+    sHi = 0u;
+  }
   const SegGeo sg = seg_geo(a, seg);
   const int64_t g = sg.g;
   const int64_t sb = sg.base + seg_begin(g, a.level, sg.n);
@@ -619,21 +628,43 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
     return w < ncd ? b.ckey[cd[w]][sb + i] : b.cidx[sb + i];
   };
 
+  // the split-dim keys of the candidates share one bin: their digits are
+  // taken relative to the smallest over the bits of their span
+  uint32_t kmin = 0xffffffffu, kmax = 0u;
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+    const uint32_t v = word(i, 0);
+    kmin = min(kmin, v);
+    kmax = max(kmax, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+    kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+  }
+  __syncthreads();  // sLo / sHi initialised
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&sLo, kmin);
+    atomicMax(&sHi, kmax);
+  }
+  __syncthreads();
+  const uint32_t klo = sLo, khi = sHi;
   uint32_t rank = r - below;
   bool unique = false;
   int w = 0;
-  uint32_t cp = 0, cm = 0;
+  uint32_t cp = 0, cm = 0, base = 0;
   for (w = 0; w < nwords && !unique; w++) {
     cp = 0;
     cm = 0;
-    for (int shift = 24; shift >= 0; shift -= 8) {
+    base = w == 0 ? klo : 0u;
+    const uint32_t span = w == 0 ? (khi >= klo ? khi - klo : 0u) : 0xffffffffu;
+    const int top = span ? ((31 - __clz(span)) & ~7) : -8;  // no digit: one value
+    for (int shift = top; shift >= 0; shift -= 8) {
       for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
       __syncthreads();
       for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
         bool ok = true;
         for (int pw_i = 0; pw_i < w && ok; pw_i++) ok = word(i, pw_i) == pw[pw_i];
         if (!ok) continue;
-        const uint32_t v = word(i, w);
+        const uint32_t v = word(i, w) - base;
         if ((v & cm) != cp) continue;
         atomicAdd(&hist[(v >> shift) & 255u], 1u);
       }
@@ -671,7 +702,7 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
         break;
       }
     }
-    if (!unique && threadIdx.x == 0) pw[w] = cp;
+    if (!unique && threadIdx.x == 0) pw[w] = cp + base;
     __syncthreads();
   }
   // w now indexes the word being matched when the pivot became unique
@@ -680,13 +711,14 @@ __global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
   if (!unique) {
     cp = pw[nwords - 1];
     cm = 0xffffffffu;
+    base = 0;
   }
   if (threadIdx.x == 0) sPivot = 0xffffffffu;
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
     bool ok = true;
     for (int pw_i = 0; pw_i < wl && ok; pw_i++) ok = word(i, pw_i) == pw[pw_i];
-    if (ok && (word(i, wl) & cm) == cp) sPivot = i;
+    if (ok && ((word(i, wl) - base) & cm) == cp) sPivot = i;
   }
   if (threadIdx.x == 0) {
     sNl = 0;
@@ -1607,7 +1639,8 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
     } else {
       CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
       const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
-      hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+      hist_kernel<SC, D><<<unsigned(int64_t(nseg) * div_up(a.chunksPerSeg, kHistGroup)), kGThreads, 0,
+                           st>>>(b, a);
       CKB_CHECK_LAUNCH();
       if (a.nb >= 512)
         select_block_kernel<<<unsigned(nseg), 256, 0, st>>>(b, a);
@@ -1835,7 +1868,8 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
     } else {
       CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
       const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
-      hist_kernel<SC, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+      hist_kernel<SC, D><<<unsigned(int64_t(nseg) * div_up(a.chunksPerSeg, kHistGroup)), kGThreads, 0,
+                           st>>>(b, a);
       CKB_CHECK_LAUNCH();
       if (a.nb >= 512)
         select_block_kernel<<<unsigned(nseg), 256, 0, st>>>(b, a);
@@ -1989,7 +2023,8 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
     } else {
       CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(L.items) * L.nb, st));
       const int64_t grid = int64_t(L.items) * L.chunksPerSeg;
-      hist_kernel<0, D><<<unsigned(grid), kGThreads, 0, st>>>(b, a);
+      hist_kernel<0, D><<<unsigned(int64_t(L.items) * div_up(L.chunksPerSeg, kHistGroup)),
+                          kGThreads, 0, st>>>(b, a);
       CKB_CHECK_LAUNCH();
       if (a.nb >= 512)
         select_block_kernel<<<unsigned(L.items), 256, 0, st>>>(b, a);
