@@ -71,7 +71,8 @@ struct BuildBufs {
   uint32_t *isSplit, *splitRank;
   // per prim position
   uint32_t *prim[2], *nodeOf[2];
-  uint32_t *fl, *fr;  // side flags -> exclusive scans
+  float *coord[2][4];  // the prim's coordinates, moved with it (SoA per dim)
+  uint32_t *fl;        // goes-left flags -> exclusive scan
   uint32_t *total;    // scan totals / pass counters [4]
   const uint8_t *data;
   int stride, poff;
@@ -108,6 +109,68 @@ __device__ inline void warp_grow(int32_t *lo, int32_t *hi, uint32_t node, bool v
   }
 }
 
+// Grows the boxes of the nodes that this CTA's valid lanes carry prims to.
+// When those nodes span fewer than kGrowSlots consecutive ids (always near
+// the root, where every warp would otherwise hit the same few boxes), the
+// warps' partial boxes are merged in shared memory first and the CTA issues
+// one global atomic per (node, dim, bound); otherwise each warp issues its
+// own (warp_grow).
+constexpr int kGrowSlots = 64;
+template <int D>
+__device__ inline void block_grow(int32_t *lo, int32_t *hi, uint32_t node, bool valid,
+                                  const float *p)
+{
+  __shared__ uint32_t nmin, nmax;
+  __shared__ int32_t slo[kGrowSlots][D], shi[kGrowSlots][D];
+  if (threadIdx.x == 0) {
+    nmin = 0xffffffffu;
+    nmax = 0u;
+  }
+  __syncthreads();
+  if (valid) {
+    atomicMin(&nmin, node);
+    atomicMax(&nmax, node);
+  }
+  __syncthreads();
+  const uint32_t n0 = nmin, n1 = nmax;
+  if (n0 > n1) return;  // no valid lane in the CTA (uniform)
+  if (n1 - n0 >= uint32_t(kGrowSlots)) {  // uniform
+    warp_grow<D>(lo, hi, node, valid, p);
+    return;
+  }
+  const int slots = int(n1 - n0) + 1;
+  for (int i = threadIdx.x; i < slots * D; i += blockDim.x) {
+    (&slo[0][0])[i] = enc(+FLT_MAX);
+    (&shi[0][0])[i] = enc(-FLT_MAX);
+  }
+  __syncthreads();
+  const unsigned active = __ballot_sync(0xffffffffu, valid);
+  if (valid) {
+    const unsigned peers = __match_any_sync(active, node);
+    const int leader = __ffs(peers) - 1;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const int32_t e = enc(p[d]);
+      const int32_t l = __reduce_min_sync(peers, e);
+      const int32_t h = __reduce_max_sync(peers, e);
+      if (lane == leader) {
+        atomicMin(&slo[node - n0][d], l);
+        atomicMax(&shi[node - n0][d], h);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < slots * D; i += blockDim.x) {
+    const int sl = i / D, d = i % D;
+    const int32_t l = slo[sl][d], h = shi[sl][d];
+    if (l <= h) {  // the slot's node received prims
+      atomicMin(&lo[int64_t(n0 + sl) * D + d], l);
+      atomicMax(&hi[int64_t(n0 + sl) * D + d], h);
+    }
+  }
+}
+
 template <int D>
 __global__ void init_kernel(BuildBufs b, int64_t n)
 {
@@ -118,11 +181,13 @@ __global__ void init_kernel(BuildBufs b, int64_t n)
     load_point<D>(b, uint32_t(i), p);
     b.prim[0][i] = uint32_t(i);
     b.nodeOf[0][i] = 0;
+#pragma unroll
+    for (int d = 0; d < D; d++) b.coord[0][d][i] = p[d];
   } else {
 #pragma unroll
     for (int d = 0; d < D; d++) p[d] = 0.f;
   }
-  warp_grow<D>(b.lo, b.hi, 0, valid, p);
+  block_grow<D>(b.lo, b.hi, 0, valid, p);
 }
 
 template <int D>
@@ -203,26 +268,17 @@ __global__ void side_kernel(BuildBufs b, int64_t n, uint32_t pb, uint32_t pe, in
   const int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p >= n) return;
   const uint32_t node = b.nodeOf[cur][p];
-  uint32_t l = 0, r = 0;
+  uint32_t l = 0;
   if (node >= pb && node < pe && b.isSplit[node - pb]) {
     const int dim = b.sdim[node];
     int side;
-    if (dim < 0) {
+    if (dim < 0)
       side = int((uint32_t(p) - b.segBegin[node]) & 1u);
-    } else {
-      float pt[D];
-      load_point<D>(b, b.prim[cur][p], pt);
-      float c = pt[0];
-#pragma unroll
-      for (int d = 1; d < D; d++)
-        if (d == dim) c = pt[d];
-      side = c >= b.spos[node];
-    }
+    else
+      side = b.coord[cur][dim][p] >= b.spos[node];
     l = side == 0;
-    r = side == 1;
   }
   b.fl[p] = l;
-  b.fr[p] = r;
 }
 
 template <int D>
@@ -246,21 +302,28 @@ __global__ void move_kernel(BuildBufs b, int64_t n, uint32_t pb, uint32_t pe, in
       const uint32_t nl = b.fl[sb + cnt] - b.fl[sb];
       const uint32_t first = b.out[node].offset;
       const bool isL = (b.fl[p + 1] - b.fl[p]) != 0;
+      // every prim of a split node goes left or right: its right-side rank
+      // is its rank in the segment minus its left-side rank
+      const uint32_t lBefore = b.fl[p] - b.fl[sb];
       if (isL) {
-        dst = sb + (b.fl[p] - b.fl[sb]);
+        dst = sb + lBefore;
         nodeOut = first;
       } else {
-        dst = sb + nl + (b.fr[p] - b.fr[sb]);
+        dst = sb + nl + (uint32_t(p) - sb - lBefore);
         nodeOut = first + 1;
       }
       moving = true;
       child = nodeOut;
-      load_point<D>(b, prim, pt);
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        pt[d] = b.coord[cur][d][p];
+        b.coord[cur ^ 1][d][dst] = pt[d];  // leaves' prims need no coordinates
+      }
     }
     b.prim[cur ^ 1][dst] = prim;
     b.nodeOf[cur ^ 1][dst] = nodeOut;
   }
-  warp_grow<D>(b.lo, b.hi, child, moving, pt);
+  block_grow<D>(b.lo, b.hi, child, moving, pt);
 }
 
 __global__ void child_counts_kernel(BuildBufs b, uint32_t pb, uint32_t pe)
@@ -348,19 +411,17 @@ int build_impl(const void *pts, int64_t n, const Layout &L, int threshold,
   for (int x = 0; x < 2; x++) {
     CKB_TRY(arena.alloc(&b.prim[x], n));
     CKB_TRY(arena.alloc(&b.nodeOf[x], n));
+    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.coord[x][d], n));
   }
   CKB_TRY(arena.alloc(&b.fl, n + 1));
-  CKB_TRY(arena.alloc(&b.fr, n + 1));
   CKB_TRY(arena.alloc(&b.total, 4));
   Node *nodesFull = nullptr;
   CKB_TRY(arena.alloc(&nodesFull, cap));
   b.out = nodesFull;
-  uint32_t *hostTotal = nullptr;
-  CKB_CUDA(cudaMallocHost(&hostTotal, sizeof(uint32_t)));
-  struct PinnedFree {
-    uint32_t *p;
-    ~PinnedFree() { cudaFreeHost(p); }
-  } pinnedGuard{hostTotal};
+  // the per-pass split count is read into pageable memory (a 4-byte copy
+  // followed by a stream sync anyway; a pinned allocation per build cost more)
+  uint32_t hostTotalVal = 0;
+  uint32_t *hostTotal = &hostTotalVal;
 
   // root: empty box, then grown by every prim (initPrims, :300-314)
   {
@@ -394,7 +455,6 @@ int build_impl(const void *pts, int64_t n, const Layout &L, int threshold,
     side_kernel<D><<<nb, 256, 0, st>>>(b, n, pb, pe, cur);
     CKB_CHECK_LAUNCH();
     CKB_TRY(exclusive_scan_u32(b.fl, b.fl, n + 1, nullptr, st, &arena));
-    CKB_TRY(exclusive_scan_u32(b.fr, b.fr, n + 1, nullptr, st, &arena));
     child_counts_kernel<<<mb, 256, 0, st>>>(b, pb, pe);
     CKB_CHECK_LAUNCH();
     move_kernel<D><<<nb, 256, 0, st>>>(b, n, pb, pe, cur);
