@@ -96,6 +96,9 @@ constexpr int kStageSpan = kChunk + 8;
 // into the global histogram with atomics (10M-point build: 1 -> 5.27 ms,
 // 4 -> 5.14 ms, 8 -> 5.23 ms)
 constexpr int kHistGroup = 4;
+// levels with at most this many subtrees resolve with 1024-thread CTAs
+// (10M-point build 5.13 -> 5.06 ms)
+constexpr int kWideResolveSegs = 16;
 // global levels whose largest subtree holds at most this many points run
 // level_fused_kernel (10M-point build: 5.61 -> 5.43 ms)
 constexpr int64_t kFusedMax = kChunk;
@@ -590,10 +593,11 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
 }
 
 // MSD radix select on the composite key among a subtree's candidates, then
-// the candidates' final placement.  One CTA per subtree.
-template <int SC, int D>
-__global__ void __launch_bounds__(kGThreads) resolve_kernel(Bufs b, LevelArgs a,
-                                                            bool explicitDims)
+// the candidates' final placement.  One CTA of NT threads per subtree: 1024
+// on the top levels, whose few subtrees have thousands of candidates each
+// (each pass is a latency-bound loop over them), 256 below.
+template <int SC, int D, int NT>
+__global__ void __launch_bounds__(NT) resolve_kernel(Bufs b, LevelArgs a, bool explicitDims)
 {
   __shared__ uint32_t hist[256];
   __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr, sLo, sHi;
@@ -1649,7 +1653,10 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
       CKB_CHECK_LAUNCH();
       partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
       CKB_CHECK_LAUNCH();
-      resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
+      if (nseg <= kWideResolveSegs)
+        resolve_kernel<SC, D, 1024><<<nseg, 1024, 0, st>>>(b, a, explicitDims);
+      else
+        resolve_kernel<SC, D, kGThreads><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
       CKB_CHECK_LAUNCH();
     }
     cb ^= 1;
@@ -1878,7 +1885,10 @@ int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, 
       CKB_CHECK_LAUNCH();
       partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
       CKB_CHECK_LAUNCH();
-      resolve_kernel<SC, D><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
+      if (nseg <= kWideResolveSegs)
+        resolve_kernel<SC, D, 1024><<<nseg, 1024, 0, st>>>(b, a, explicitDims);
+      else
+        resolve_kernel<SC, D, kGThreads><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
       CKB_CHECK_LAUNCH();
     }
     cb ^= 1;
@@ -2033,7 +2043,10 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
       CKB_CHECK_LAUNCH();
       partition_kernel<0, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
       CKB_CHECK_LAUNCH();
-      resolve_kernel<0, D><<<unsigned(L.items), kGThreads, 0, st>>>(b, a, false);
+      if (L.items <= kWideResolveSegs)
+        resolve_kernel<0, D, 1024><<<unsigned(L.items), 1024, 0, st>>>(b, a, false);
+      else
+        resolve_kernel<0, D, kGThreads><<<unsigned(L.items), kGThreads, 0, st>>>(b, a, false);
       CKB_CHECK_LAUNCH();
     }
     cb ^= 1;
