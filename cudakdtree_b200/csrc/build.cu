@@ -1169,6 +1169,7 @@ __device__ void sub_radix_sort_all(SubSmem<D, TILE, NT> &S, int m)
         const uint32_t dg = valid ? ((S.key[d][src[i]] - kmin[d]) >> shift) & 255u : 256u + lane;
         const uint32_t peers = __match_any_sync(0xffffffffu, dg);
         if (valid && (peers & ltMask) == 0) S.rh[d][wid][dg] += uint16_t(__popc(peers));
+        __syncwarp();  // the next round's leaders read these counts
       }
     }
     __syncthreads();
