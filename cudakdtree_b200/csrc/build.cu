@@ -24,12 +24,14 @@
 //                     candidates to the children, derives the children's
 //                     domain boxes and split dims (widest extent of the
 //                     domain box, box.h:112-125, builder_thrust.h:238-306)
+//    Once a level's subtrees fit one staged chunk (kFusedMax points),
+//    level_fused_kernel does all four steps with one CTA per subtree.
 //  subtree phase -- one CTA per subtree of <= kTile points, all remaining
 //    levels in shared memory: one index list per dimension is sorted once
 //    by coordinate; per level the pivot is read from the list of the
 //    level's dim at rank leftSize (an equal-coordinate run around it is
 //    ranked by the composite key), and all lists are stably partitioned
-//    with block-wide scans.
+//    with warp ballots and a block-wide scan of their counts.
 //  finalize_kernel -- gathers the caller's records into node order and
 //    writes the explicit split dims.
 //
