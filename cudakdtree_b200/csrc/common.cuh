@@ -74,6 +74,10 @@ struct TempArena {
     bytes = (bytes + 255) & ~size_t(255);
     if (mem && mem->alloc) {
       if (mem->alloc(mem->ctx, &p, bytes, stream) != 0 || !p) return CUKD_ERR_OUT_OF_MEMORY;
+      if (reinterpret_cast<uintptr_t>(p) & 15u) {  // bulk copies need 16-byte alignment
+        if (mem->release) mem->release(mem->ctx, p, stream);
+        return CUKD_ERR_INVALID_ARGUMENT;
+      }
     } else {
       cudaError_t e = cudaMallocAsync(&p, bytes, stream);
       if (e != cudaSuccess) {

@@ -83,7 +83,10 @@ typedef struct cukd_layout {
 /* world bounds: box_t<point_t> (cukd/box.h:35-82) = lower[num_dims] then
  * upper[num_dims], of the scalar type. */
 
-/* Memory resource: reference GpuMemoryResource (cukd/helpers.h:30-33). */
+/* Memory resource: reference GpuMemoryResource (cukd/helpers.h:30-33).
+ * Blocks must be at least 16-byte aligned (cudaMalloc-style allocators give
+ * 256; the builder stages its arrays with 16-byte bulk copies): a misaligned
+ * block makes the call return CUKD_ERR_INVALID_ARGUMENT. */
 typedef struct cukd_mem_resource {
   void *ctx;
   int (*alloc)(void *ctx, void **ptr, size_t bytes, cudaStream_t stream); /* 0 = ok */

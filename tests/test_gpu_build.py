@@ -197,3 +197,37 @@ def test_partition_staging_waits_never_give_up():
     count = ctypes.c_uint(7)
     assert ck.lib().cukd_async_wait_timeouts(ctypes.byref(count)) == 0
     assert count.value == 0
+
+
+def test_misaligned_memory_resource_is_rejected_before_any_launch():
+    """A caller memory resource must hand out 16-byte-aligned blocks (the
+    partition pass stages them with bulk copies); a block 4 bytes off is
+    refused with CUKD_ERR_INVALID_ARGUMENT before any kernel runs, and the
+    points are left untouched."""
+    import ctypes as C
+    live = {}
+
+    def alloc(ctx, out, nbytes, stream):
+        t = torch.empty(int(nbytes) + 64, dtype=torch.uint8, device="cuda")
+        p = t.data_ptr() + 4
+        live[p] = t
+        out[0] = p
+        return 0
+
+    def release(ctx, ptr, stream):
+        live.pop(ptr, None)
+        return 0
+
+    a_fn = ck._ALLOC_FN(alloc)
+    r_fn = ck._RELEASE_FN(release)
+    mr = ck.MemResource(None, C.cast(a_fn, C.c_void_p), C.cast(r_fn, C.c_void_p))
+    n = 5000
+    pts = make_points(n, 3, "uniform", seed=11)
+    t = torch.from_numpy(pts).cuda()
+    before = t.clone()
+    lay = ck.layout_for("float32", 3)
+    rc = ck.lib().cukd_build_tree(t.data_ptr(), n, C.byref(lay), None, 0, None, C.byref(mr))
+    torch.cuda.synchronize()
+    assert rc == 1  # CUKD_ERR_INVALID_ARGUMENT
+    assert torch.equal(t, before)
+    assert not live  # the misaligned block was handed back
