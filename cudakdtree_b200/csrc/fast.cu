@@ -27,224 +27,20 @@
 //     answers every queued query, in its own order);
 //   - the candidate list is d2-only floats + ids in registers (right-aligned
 //     k+1 live slots in KC registers), no 64-bit compares;
+//   - far-child stack entries of 12 bytes (node + bf16-truncated squared
+//     offsets of the box's closest point, fast_one.cuh);
 //   - optional per-query initial cull radius (learned radius proposal).
 #include <algorithm>
 
 #include "common.cuh"
 #include "fast.cuh"
+#include "fast_one.cuh"
 
 namespace ckb {
 namespace fast {
 
 using query::QArgs;
 using query::TreeView;
-
-// One thread per query (queries in Morton order).  Culling uses the
-// closest-corner distance of each subtree's domain box, the bound of
-// traverse_cct (traverse-cct.h:25-99): the far child's box differs from its
-// parent's only in the split dim, so its closest point to the query is the
-// parent's with that coordinate set to the split value.  Corner distances
-// never exceed the distance of any point inside (every term is a rounded
-// difference of a smaller magnitude), so "<=" culling sees every point with
-// d2 <= the final (k+1)-th distance.
-template <int D, bool EXPL, bool VEC16, int KC>
-__device__ __forceinline__ void knn_fast_one(const FastArgs &fa, int64_t i)
-{
-  const QArgs &a = fa.q;
-  const int64_t myq = a.order ? int64_t(a.order[i]) : i;
-  const TreeView tv = query::tree_of<D, 4>(a, myq);
-  const int N = int(tv.n);
-  const int k = fa.kk;  // live slots: k+1, right-aligned
-  const uint8_t *tree = tv.tree;
-
-  float q[D];
-  {
-    const float *qp = (const float *)a.queries + myq * D;
-#pragma unroll
-    for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
-  }
-  float r2 = __fmul_rn(a.cutoff, a.cutoff);
-  if (fa.radius) {
-    const float rr = __fmul_rn(__ldg(fa.radius + myq), fa.radius_scale);
-    const float rb = __fmul_rn(rr, rr);
-    r2 = rb < r2 ? rb : r2;
-  }
-  const float r2init = r2;
-  float e[KC];
-  int id[KC];
-#pragma unroll
-  for (int j = 0; j < KC; j++) {
-    e[j] = j < KC - (k + 1) ? -1.f : r2;
-    id[j] = -1;
-  }
-  float cull = r2;
-  bool sawInit = false;
-  int visits = 0;
-
-  // closest point of the root's box (the world bounds, or all of space)
-  float closest[D];
-  const float *bnd = (const float *)tv.bounds;
-#pragma unroll
-  for (int d = 0; d < D; d++) {
-    float v = q[d];
-    if (bnd) {
-      const float lo = __ldg(bnd + d), hi = __ldg(bnd + D + d);
-      v = v < lo ? lo : v;
-      v = hi < v ? hi : v;
-    }
-    closest[d] = v;
-  }
-  auto dist2 = [&](const float *c) {
-    float s = __fmul_rn(__fsub_rn(c[0], q[0]), __fsub_rn(c[0], q[0]));
-#pragma unroll
-    for (int d = 1; d < D; d++) s = __fadd_rn(s, __fmul_rn(__fsub_rn(c[d], q[d]), __fsub_rn(c[d], q[d])));
-    return s;
-  };
-
-  // far-child stack: node, its box's closest point and that point's d2
-  // (a culled entry is dropped on one load, without recomputing)
-  int nodeSt[32];
-  float cornerSt[32][D];
-  float cornerD2[32];
-  int sp = 0;
-  int curr = (N > 0 && dist2(closest) <= cull) ? 0 : N;
-  for (;;) {
-    if (curr >= N) {
-      bool found = false;
-      while (sp > 0) {
-        --sp;
-        if (cornerD2[sp] <= cull) {
-#pragma unroll
-          for (int d = 0; d < D; d++) closest[d] = cornerSt[sp][d];
-          curr = nodeSt[sp];
-          found = true;
-          break;
-        }
-      }
-      if (!found) break;
-    }
-    float p[D];
-    int dim;
-    if (VEC16) {
-      const uint4 v = __ldg((const uint4 *)(tree + int64_t(curr) * 16));
-      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int d = 0; d < D; d++) p[d] = __uint_as_float(w[d]);
-      dim = EXPL ? int((w[3] >> a.dshift) & a.dmask) : (level_of(curr) % D);
-    } else {
-      const float *c = (const float *)(tree + int64_t(curr) * a.stride + a.poff);
-#pragma unroll
-      for (int d = 0; d < D; d++) p[d] = __ldg(c + d);
-      dim = EXPL ? int((__ldg((const uint32_t *)(tree + int64_t(curr) * a.stride + a.doff)) >>
-                        a.dshift) & a.dmask)
-                 : (level_of(curr) % D);
-    }
-    const float d2 = dist2(p);
-    ++visits;
-    sawInit |= (d2 == r2init);
-    if (d2 < e[KC - 1]) {
-      // insert d2 into the ascending list, dropping the largest: each slot
-      // is computed from its two old neighbours, with no dependency chain
-      // through the list (with the stored corner d2 above: 20.3 -> 18.8 ms
-      // at k = 16 on the 10M-point benchmark)
-#pragma unroll
-      for (int j = KC - 1; j >= 0; j--) {
-        const bool lt = d2 < e[j];
-        const bool ltBelow = j > 0 ? (d2 < e[j - 1]) : false;
-        const float below = j > 0 ? e[j - 1] : 0.f;
-        const int belowId = j > 0 ? id[j - 1] : 0;
-        e[j] = ltBelow ? below : (lt ? d2 : e[j]);
-        id[j] = ltBelow ? belowId : (lt ? curr : id[j]);
-      }
-      cull = e[KC - 1];
-    }
-    float nodeC = p[0], queryC = q[0];
-#pragma unroll
-    for (int d = 1; d < D; d++)
-      if (d == dim) {
-        nodeC = p[d];
-        queryC = q[d];
-      }
-    const bool leftIsClose = queryC < nodeC;
-    const int lChild = 2 * curr + 1;
-    const int farChild = leftIsClose ? lChild + 1 : lChild;
-    if (farChild < N) {
-      float fc[D];
-#pragma unroll
-      for (int d = 0; d < D; d++) fc[d] = d == dim ? nodeC : closest[d];
-      const float fd2 = dist2(fc);
-      if (fd2 <= cull) {
-#pragma unroll
-        for (int d = 0; d < D; d++) cornerSt[sp][d] = fc[d];
-        cornerD2[sp] = fd2;
-        nodeSt[sp] = farChild;
-        sp++;
-      }
-    }
-    curr = leftIsClose ? lChild : lChild + 1;
-  }
-
-  // ---- decide: answer now, or queue for the reference-order traversal
-  const float X = e[KC - 2];  // k-th smallest d2
-  const float Y = e[KC - 1];  // (k+1)-th smallest d2
-  const int idX = id[KC - 2];
-  bool ok;
-  if (fa.fcp) {
-    // unique minimum, or nothing below the cut-off (strict '<' in FCPResult)
-    ok = idX < 0 ? !fa.radius : (Y > X);
-  } else if (idX >= 0) {
-    ok = Y > X;  // strict gap at the k-th boundary
-  } else {
-    ok = !fa.radius && !sawInit;  // fewer than k inside the cut-off
-  }
-  if (!(X == X)) ok = false;  // NaN coordinates
-  if (a.visits) a.visits[myq] += visits;  // accumulated over chained passes
-  if (!ok) {
-    const int slot = atomicAdd(fa.fb_count, 1);
-    fa.fb_list[slot] = int32_t(myq);
-    if (fa.status) fa.status[myq] = 1;
-    return;
-  }
-  if (fa.status) fa.status[myq] = 0;
-  if (fa.fcp) {
-    if (a.out_ids) a.out_ids[myq] = idX >= 0 ? idX : -1;
-    if (a.out_d2) ((float *)a.out_d2)[myq] = idX >= 0 ? X : r2init;
-    return;
-  }
-  // the list is sorted by d2; equal-d2 entries must be ordered by id like
-  // the reference's (d2, id) keys -- rare, sorted only when present
-  unsigned long long key[KC];
-  bool anyEq = false;
-#pragma unroll
-  for (int j = 0; j < KC; j++) {
-    const bool live = j >= KC - 1 - k && j < KC - 1;
-    key[j] = live ? ((unsigned long long)__float_as_uint(e[j]) << 32) | uint32_t(id[j]) : ~0ull;
-    if (live && j + 1 < KC - 1) anyEq |= (e[j] == e[j + 1]);
-  }
-  if (anyEq) {
-#pragma unroll
-    for (int pass = 0; pass < KC; pass++) {
-#pragma unroll
-      for (int j = (pass & 1); j + 1 < KC; j += 2) {
-        const unsigned long long x = key[j], y = key[j + 1];
-        key[j] = x < y ? x : y;
-        key[j + 1] = x < y ? y : x;
-      }
-    }
-  }
-  const int off = anyEq ? 0 : KC - 1 - k;
-  int32_t *oid = a.out_ids ? a.out_ids + myq * k : nullptr;
-  float *od = a.out_d2 ? (float *)a.out_d2 + myq * k : nullptr;
-#pragma unroll
-  for (int j = 0; j < KC; j++) {
-    const int o = j - off;
-    if (o >= 0 && o < k) {
-      if (oid) oid[o] = int32_t(uint32_t(key[j]));
-      if (od) od[o] = __uint_as_float(uint32_t(key[j] >> 32));
-    }
-  }
-  if (a.out_max) ((float *)a.out_max)[myq] = X;
-}
 
 // Register cap: at most 64 registers (4 resident 256-thread blocks per SM)
 // for lists of up to 17 slots in 2-D / 3-D (9 in 4-D), 128 otherwise.  The
@@ -256,8 +52,12 @@ __global__ void __launch_bounds__(256, ((KC <= 9 || (KC <= 17 && D <= 3)) ? 4 : 
 {
   const int64_t limit = fa.q.count_ptr ? int64_t(*fa.q.count_ptr) : fa.q.nq;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < limit;
-       i += int64_t(gridDim.x) * blockDim.x)
-    knn_fast_one<D, EXPL, VEC16, KC>(fa, i);
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t myq = fa.q.order ? int64_t(fa.q.order[i]) : i;
+    const bool seeded = fa.radius != nullptr;
+    const float r = seeded ? __ldg(fa.radius + myq) : 0.f;
+    knn_fast_one<D, EXPL, VEC16, KC>(fa, i, myq, seeded, r);
+  }
 }
 
 // Large k (k + 1 > 33): the same corner-culled traversal keeping the k+1

@@ -8,11 +8,14 @@
 //     f (4) -> 64 ReLU -> 64 ReLU -> 1   (the log of the distance,
 //                                         standardised over the training set)
 // Weights are kept in BF16 for every forward/backward pass (FP32 master
-// copy for the optimiser), arithmetic accumulates in FP32.  Training uses
+// copy for the optimiser); the inputs and the first hidden layer enter the
+// products as bf16, and every sum accumulates in FP32.  Training uses
 // exact k-th distances the plain traversal computes, Adam, minibatches.
 //
-// Inference feeds the fast exact kernel (fast.cu) a per-query initial cull
-// radius r_hat * scale.  A query that finds at least k points strictly
+// The learned kNN predicts each query's radius inside its search kernel
+// (knn_learned_kernel: the network on the tensor cores, then the fast exact
+// traversal of fast_one.cuh from an initial cull radius r_hat * scale).
+// A query that finds at least k points strictly
 // inside that radius has its exact answer (every point nearer than its k-th
 // neighbour was examined); any other query -- fewer than k inside, or a
 // distance tie at the k-th boundary -- is re-run by the plain unbounded
@@ -26,7 +29,10 @@
 //                       CTA; per-CTA gradient sums merged with atomics
 //   adam_kernel         Adam update of the FP32 master weights, refresh of
 //                       the BF16 copy, gradient reset
-//   infer_kernel        forward pass per query -> radius
+//   infer_kernel        forward pass of 32 queries per warp on the tensor
+//                       cores (mma.sync bf16, FP32 accumulate) -> radius
+//   knn_learned_kernel  the same forward pass fused with the seeded kNN
+//                       traversal (pass 1 of cukd_knn_learned)
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -35,6 +41,8 @@
 
 #include "common.cuh"
 #include "fast.cuh"
+#include "fast_one.cuh"
+#include "learned.cuh"
 #include "query.cuh"
 
 struct cukd_radius_model_s;
@@ -42,66 +50,17 @@ struct cukd_radius_model_s;
 namespace ckb {
 namespace learned {
 
-constexpr int H = 64;
-constexpr int OW1 = 0;            // [H][4]  W1[j][i]
-constexpr int OB1 = OW1 + 4 * H;  // [H]
-constexpr int OW2 = OB1 + H;      // [H][H]  W2[j][k]: output j, input k
-constexpr int OB2 = OW2 + H * H;  // [H]
-constexpr int OW3 = OB2 + H;      // [H]
-constexpr int OB3 = OW3 + H;      // [1]
-constexpr int NP = OB3 + 1;       // 4545 parameters
 constexpr int S = 32;             // samples per CTA in training
 constexpr int kTrainThreads = 256;
-
-struct Norm {
-  float lo[3], invext[3];
-  int res;
-  float invLogMax;  // 1 / log(1 + max cell count)
-  float tmean, tstd;
-};
 
 struct ModelDev {
   float *params;          // FP32 master
   __nv_bfloat16 *wbf;     // BF16 copy used by every pass
   float *m, *v, *grad;    // Adam state, gradient accumulator
   uint32_t *grid;         // res^3 counts
+  float *dens;            // res^3 log1pf(count): the density feature's cells
   float *loss;            // per-step loss sums
 };
-
-// log(1 + cell count), trilinearly interpolated between the centres of the
-// 8 cells around the query (a smooth density estimate at grid scale)
-__device__ inline void features(const Norm &nm, const uint32_t *grid, const float *q, float *f)
-{
-  int c0[3];
-  float w[3];
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const float u = __fmul_rn(__fsub_rn(q[d], nm.lo[d]), nm.invext[d]);
-    f[d] = __fsub_rn(__fmul_rn(u, 2.f), 1.f);
-    // position in cell-centre coordinates
-    float c = __fsub_rn(__fmul_rn(u, float(nm.res)), 0.5f);
-    c = fminf(fmaxf(c, 0.f), float(nm.res - 1));
-    int ci = int(c);
-    ci = ci < nm.res - 1 ? ci : nm.res - 1;
-    c0[d] = ci;
-    w[d] = __fsub_rn(c, float(ci));
-  }
-  float acc = 0.f;
-#pragma unroll
-  for (int corner = 0; corner < 8; corner++) {
-    int cell = 0;
-    float wt = 1.f;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const int bit = (corner >> d) & 1;
-      const int ci = min(c0[d] + bit, nm.res - 1);
-      cell = cell * nm.res + ci;
-      wt = __fmul_rn(wt, bit ? w[d] : __fsub_rn(1.f, w[d]));
-    }
-    acc = __fmaf_rn(wt, log1pf(float(__ldg(grid + cell))), acc);
-  }
-  f[3] = __fmul_rn(acc, nm.invLogMax);
-}
 
 // ---------------------------------------------------------------------------
 __global__ void grid_count_kernel(const uint8_t *__restrict__ pts, int64_t n, int stride,
@@ -121,6 +80,13 @@ __global__ void grid_count_kernel(const uint8_t *__restrict__ pts, int64_t n, in
   }
 }
 
+__global__ void density_kernel(const uint32_t *grid, int64_t cells, float *dens)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < cells;
+       i += int64_t(gridDim.x) * blockDim.x)
+    dens[i] = log1pf(float(grid[i]));
+}
+
 __global__ void grid_max_kernel(const uint32_t *grid, int64_t cells, uint32_t *out)
 {
   uint32_t m = 0;
@@ -132,13 +98,13 @@ __global__ void grid_max_kernel(const uint32_t *grid, int64_t cells, uint32_t *o
 }
 
 __global__ void features_kernel(const float *__restrict__ q, int64_t nq, Norm nm,
-                                const uint32_t *grid, float *feat)
+                                const float *dens, float *feat)
 {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nq) return;
   float qq[3] = {q[i * 3], q[i * 3 + 1], q[i * 3 + 2]};
   float f[4];
-  features(nm, grid, qq, f);
+  features(nm, dens, qq, f);
 #pragma unroll
   for (int d = 0; d < 4; d++) feat[i * 4 + d] = f[d];
 }
@@ -189,7 +155,7 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
   const int ns = left <= 0 ? 0 : (left < S ? int(left) : S);
   for (int i = tid; i < S * 4; i += kTrainThreads) {
     const int s = i / 4;
-    M.f[s][i % 4] = s < ns ? feat[(s0 + s) * 4 + i % 4] : 0.f;
+    M.f[s][i % 4] = s < ns ? bf16_round(feat[(s0 + s) * 4 + i % 4]) : 0.f;
   }
   __syncthreads();
   if (ns == 0) return;
@@ -199,7 +165,7 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
     float z = M.b1[j];
 #pragma unroll
     for (int c = 0; c < 4; c++) z = __fmaf_rn(M.w1[j][c], M.f[s][c], z);
-    M.h1[s][j] = fmaxf(z, 0.f);
+    M.h1[s][j] = bf16_round(fmaxf(z, 0.f));  // as the tensor cores see it
   }
   __syncthreads();
   // layer 2
@@ -283,45 +249,75 @@ __global__ void adam_kernel(float *params, __nv_bfloat16 *wbf, float *m, float *
 }
 
 // ---------------------------------------------------------------------------
-// inference: one thread per query
+// inference: 32 queries per warp through mlp_forward_warp (tensor cores)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) infer_kernel(const __nv_bfloat16 *__restrict__ wbf,
+__global__ void __launch_bounds__(128, 4) infer_kernel(const __nv_bfloat16 *__restrict__ wbf,
                                                     const float *__restrict__ q, int64_t nq,
-                                                    Norm nm, const uint32_t *grid,
-                                                    float *radius)
+                                                    Norm nm, const float *dens, float *radius)
 {
-  __shared__ float w1[H][4], b1[H], w2[H][H], b2[H], w3[H], b3;
-  for (int i = threadIdx.x; i < NP; i += blockDim.x) {
-    const float w = __bfloat162float(wbf[i]);
-    if (i < OB1) w1[(i - OW1) / 4][(i - OW1) % 4] = w;
-    else if (i < OW2) b1[i - OB1] = w;
-    else if (i < OB2) w2[(i - OW2) / H][(i - OW2) % H] = w;
-    else if (i < OW3) b2[i - OB2] = w;
-    else if (i < OB3) w3[i - OW3] = w;
-    else b3 = w;
-  }
-  __syncthreads();
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= nq) return;
-  float qq[3] = {__ldg(q + i * 3), __ldg(q + i * 3 + 1), __ldg(q + i * 3 + 2)};
+  if (i - (threadIdx.x & 31) >= nq) return;  // whole warps only: they run the mma together
+  const bool live = i < nq;
+  const int64_t qi = live ? i : 0;
+  const float qq[3] = {__ldg(q + qi * 3), __ldg(q + qi * 3 + 1), __ldg(q + qi * 3 + 2)};
   float f[4];
-  features(nm, grid, qq, f);
-  float h1[H];
-#pragma unroll
-  for (int j = 0; j < H; j++) {
-    float z = b1[j];
-#pragma unroll
-    for (int c = 0; c < 4; c++) z = __fmaf_rn(w1[j][c], f[c], z);
-    h1[j] = fmaxf(z, 0.f);
+  features(nm, dens, qq, f);
+  const float y = mlp_forward_warp(wbf, f);
+  if (live) radius[i] = expf(__fmaf_rn(y, nm.tstd, nm.tmean));
+}
+
+// ---------------------------------------------------------------------------
+// Pass 1 of the learned kNN, fused: each warp predicts the radii of 32
+// consecutive queries of the visiting order on the tensor cores, then every
+// lane runs the fast traversal (fast_one.cuh) of its query from its radius.
+// The prediction never leaves registers; the traversal is latency-bound, so
+// the network's instructions mostly fill issue slots the traversal leaves
+// idle.
+// ---------------------------------------------------------------------------
+template <bool EXPL, bool VEC16, int KC>
+__global__ void __launch_bounds__(256, KC <= 17 ? 4 : 2)
+    knn_learned_kernel(fast::FastArgs fa, const __nv_bfloat16 *__restrict__ wbf,
+                       const float *__restrict__ dens, Norm nm)
+{
+  const int lane = threadIdx.x & 31;
+  const int64_t nq = fa.q.nq;
+  const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < nq;
+       w += warps) {
+    const int64_t i = w * 32 + lane;
+    const bool live = i < nq;
+    // lanes past the end (last warp) predict query 0's radius and stop
+    const int64_t myq = live ? (fa.q.order ? int64_t(__ldg(fa.q.order + i)) : i) : 0;
+    const float *qp = (const float *)fa.q.queries + myq * 3;
+    const float qq[3] = {__ldg(qp), __ldg(qp + 1), __ldg(qp + 2)};
+    float f[4];
+    features(nm, dens, qq, f);
+    __syncwarp();
+    const float y = mlp_forward_warp(wbf, f);
+    const float r = expf(__fmaf_rn(y, nm.tstd, nm.tmean));
+    if (live) fast::knn_fast_one<3, EXPL, VEC16, KC>(fa, i, myq, true, r);
   }
-  float y = b3;
-  for (int j = 0; j < H; j++) {
-    float z = b2[j];
-#pragma unroll
-    for (int c = 0; c < H; c++) z = __fmaf_rn(w2[j][c], h1[c], z);
-    y = __fmaf_rn(w3[j], fmaxf(z, 0.f), y);
-  }
-  radius[i] = expf(__fmaf_rn(y, nm.tstd, nm.tmean));
+}
+
+template <bool EXPL, bool VEC16>
+int launch_learned(const fast::FastArgs &fa, const __nv_bfloat16 *wbf, const float *dens,
+                   const Norm &nm, cudaStream_t st)
+{
+  const int bs = 256;
+  const unsigned grid = unsigned(std::max<int64_t>(1, div_up(fa.q.nq, bs)));
+  const int slots = fa.kk + 1;
+  if (slots <= 5)
+    knn_learned_kernel<EXPL, VEC16, 5><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+  else if (slots <= 9)
+    knn_learned_kernel<EXPL, VEC16, 9><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+  else if (slots <= 17)
+    knn_learned_kernel<EXPL, VEC16, 17><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+  else if (slots <= 33)
+    knn_learned_kernel<EXPL, VEC16, 33><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+  else
+    return CUKD_ERR_UNSUPPORTED;
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
 }
 
 // deterministic initialisation (He-uniform), a 64-bit LCG seeded by the caller
@@ -365,6 +361,7 @@ static int model_alloc(cukd_radius_model_s *m, int res)
   CKB_CUDA(cudaMalloc(&m->d.v, sizeof(float) * NP));
   CKB_CUDA(cudaMalloc(&m->d.grad, sizeof(float) * NP));
   CKB_CUDA(cudaMalloc(&m->d.grid, sizeof(uint32_t) * size_t(res) * res * res));
+  CKB_CUDA(cudaMalloc(&m->d.dens, sizeof(float) * size_t(res) * res * res));
   CKB_CUDA(cudaMalloc(&m->d.loss, sizeof(float) * 2));
   return CUKD_OK;
 }
@@ -401,7 +398,8 @@ int cukd_radius_model_destroy(cukd_radius_model *model)
   auto *m = (cukd_radius_model_s *)model;
   if (!m) return CUKD_OK;
   for (void *p : {(void *)m->d.params, (void *)m->d.wbf, (void *)m->d.m, (void *)m->d.v,
-                  (void *)m->d.grad, (void *)m->d.grid, (void *)m->d.loss})
+                  (void *)m->d.grad, (void *)m->d.grid, (void *)m->d.dens,
+                  (void *)m->d.loss})
     if (p) cudaFree(p);
   delete m;
   return CUKD_OK;
@@ -432,6 +430,9 @@ int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_points, i
   uint32_t *mx = nullptr;
   CKB_CUDA(cudaMallocAsync(&mx, sizeof(uint32_t), st));
   CKB_CUDA(cudaMemsetAsync(mx, 0, sizeof(uint32_t), st));
+  density_kernel<<<std::max<int64_t>(1, std::min<int64_t>(div_up(cells, 256), 1024)), 256, 0,
+                   st>>>(m->d.grid, cells, m->d.dens);
+  CKB_CHECK_LAUNCH();
   grid_max_kernel<<<std::max<int64_t>(1, std::min<int64_t>(div_up(cells, 256), 1024)), 256, 0,
                     st>>>(m->d.grid, cells, mx);
   CKB_CHECK_LAUNCH();
@@ -457,7 +458,7 @@ int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
   CKB_TRY(arena.alloc(&feat, nq * 4));
   CKB_TRY(arena.alloc(&tgt, nq));
   const unsigned nb = unsigned(div_up(nq, 256));
-  features_kernel<<<nb, 256, 0, st>>>(d_queries, nq, m->norm, m->d.grid, feat);
+  features_kernel<<<nb, 256, 0, st>>>(d_queries, nq, m->norm, m->d.dens, feat);
   CKB_CHECK_LAUNCH();
   targets_kernel<<<nb, 256, 0, st>>>(d_kth_d2, nq, tgt);
   CKB_CHECK_LAUNCH();
@@ -512,7 +513,7 @@ int cukd_radius_model_predict(const cukd_radius_model *model, const float *d_que
   if (!m || (nq > 0 && (!d_queries || !d_out_radius))) return CUKD_ERR_INVALID_ARGUMENT;
   if (nq == 0) return CUKD_OK;
   infer_kernel<<<unsigned(div_up(nq, 128)), 128, 0, st>>>(m->d.wbf, d_queries, nq, m->norm,
-                                                          m->d.grid, d_out_radius);
+                                                          m->d.dens, d_out_radius);
   CKB_CHECK_LAUNCH();
   return CUKD_OK;
 }
@@ -557,7 +558,7 @@ int cukd_radius_model_features(const cukd_radius_model *model, const float *d_qu
   auto *m = (const cukd_radius_model_s *)model;
   if (!m || nq < 0) return CUKD_ERR_INVALID_ARGUMENT;
   if (nq == 0) return CUKD_OK;
-  features_kernel<<<unsigned(div_up(nq, 256)), 256, 0, st>>>(d_queries, nq, m->norm, m->d.grid,
+  features_kernel<<<unsigned(div_up(nq, 256)), 256, 0, st>>>(d_queries, nq, m->norm, m->d.dens,
                                                               d_out_features);
   CKB_CHECK_LAUNCH();
   return CUKD_OK;
@@ -584,9 +585,6 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   if (nq == 0) return CUKD_OK;
   if (!d_queries || !d_out_ids || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;
   TempArena arena(st, mem);
-  float *radius = nullptr;
-  CKB_TRY(arena.alloc(&radius, nq));
-  CKB_TRY(cukd_radius_model_predict(model, (const float *)d_queries, nq, radius, st));
   query::QArgs a = {};
   a.tree = (const uint8_t *)d_tree;
   a.n = n;
@@ -618,20 +616,26 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   int32_t *fb1 = nullptr, *fb2 = nullptr;
   CKB_TRY(arena.alloc(&fb1, nq));
   CKB_TRY(arena.alloc(&fb2, nq));
-  // pass 1: learned initial radius
+  // pass 1: radii predicted and searched in one kernel
   fast::FastArgs fa = {};
   fa.q = a;
   fa.kk = p->k;
   fa.work = ctr;
   fa.fb_count = ctr + 1;
   fa.fb_list = fb1;
-  fa.radius = radius;
   fa.radius_scale = radius_scale;
   fa.status = d_status;
-  CKB_TRY(run_fast(fa, 3, st));
+  {
+    const bool expl = L.doff >= 0;
+    const bool vec16 = L.stride == 16 && L.poff == 0 && (!expl || L.doff == 12);
+    const int rc = expl ? (vec16 ? launch_learned<true, true>(fa, m->d.wbf, m->d.dens, m->norm, st)
+                                 : launch_learned<true, false>(fa, m->d.wbf, m->d.dens, m->norm, st))
+                        : (vec16 ? launch_learned<false, true>(fa, m->d.wbf, m->d.dens, m->norm, st)
+                                 : launch_learned<false, false>(fa, m->d.wbf, m->d.dens, m->norm, st));
+    CKB_TRY(rc);
+  }
   // pass 2: plain unbounded traversal of the queries pass 1 could not answer
   fast::FastArgs fb = fa;
-  fb.radius = nullptr;
   fb.status = nullptr;
   fb.q.order = fb1;
   fb.q.count_ptr = ctr + 1;

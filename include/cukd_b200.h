@@ -6,7 +6,8 @@
  * the plain-C, status-returning counterpart of one of its host templates
  * (cited per declaration, paths relative to the reference project).  The
  * C++ shim in include/cukd/ keeps the reference's template API and forwards
- * here; see INTEGRATION.md for the ctypes / C++ bindings.
+ * here; Python reaches the same entry points through ctypes
+ * (cudakdtree_b200/__init__.py).
  *
  * Conventions
  *   - All pointers named d_* are device pointers (cudaMalloc'd or managed).
@@ -392,7 +393,10 @@ CUKD_API int cukd_radius_model_gradients(cukd_radius_model *model, const float *
                                          float *h_params_bf16, float *h_loss,
                                          cudaStream_t stream);
 
-/* kNN (k = 2..32) seeded with the learned radius times radius_scale.
+/* kNN (k = 2..32) seeded with the learned radius times radius_scale: the
+ * queries are put in Morton order, the network predicts their radii in that
+ * order on the tensor cores, and the candidate-list traversal starts each
+ * query's cull radius at its prediction.
  * d_out_fallback (optional, device int[2]): queries re-run by the plain
  * traversal, and by the reference's own visiting order.  d_status
  * (optional, device int[nq]): 0 if the learned pass answered the query, 1 if

@@ -218,6 +218,103 @@ int cko_build(int scalar, int D, const void *coords, int64_t n, int explicit_dim
 }
 
 /* ===================================================================== */
+/* canonical-tree check (the build's defining property, at any size)      */
+/* ===================================================================== */
+
+/* The reference's builders (builder_thrust.h:414-512, :514-601) stable-sort
+ * every subtree's points by the split coordinate, so inside the subtree of
+ * node a they are ordered by the composite key
+ *     (c[dim(a)], c[dim(parent(a))], ..., c[dim(root)], input index)
+ * and a holds the point of rank leftSize(a).  With the left-balanced sizes
+ * fixed, a tree is the canonical one exactly when, for every node a, every
+ * point of its left subtree has a smaller composite key than a's point and
+ * every point of its right subtree a larger one; with explicit dims each
+ * node's dim must also be the widest extent of its domain box (the world
+ * bounds clipped by the ancestors' planes, box.h:112-125).  Checking this
+ * costs O(n log n) and no sort, so it scales to trees the recursive build
+ * above is too slow for. */
+typedef struct {
+  int scalar, D;
+  const float *cf;
+  const int32_t *ci;
+  const int64_t *index;
+  const int32_t *dims;
+} check_ctx;
+
+static inline int node_dim(const check_ctx *c, int64_t a)
+{
+  return c->dims ? c->dims[a] : level_of(a) % c->D;
+}
+
+static inline int coord_cmp(const check_ctx *c, int64_t i, int64_t a, int d)
+{
+  if (c->scalar == 0) {
+    const float x = c->cf[i * c->D + d], y = c->cf[a * c->D + d];
+    return x < y ? -1 : (y < x ? 1 : 0);
+  }
+  const int32_t x = c->ci[i * c->D + d], y = c->ci[a * c->D + d];
+  return x < y ? -1 : (y < x ? 1 : 0);
+}
+
+/* sign of key(i) - key(a) in node a's composite order */
+static int composite_cmp(const check_ctx *c, int64_t i, int64_t a)
+{
+  for (int64_t anc = a;; anc = (anc - 1) / 2) {
+    const int r = coord_cmp(c, i, a, node_dim(c, anc));
+    if (r) return r;
+    if (anc == 0) break;
+  }
+  return c->index[i] < c->index[a] ? -1 : (c->index[a] < c->index[i] ? 1 : 0);
+}
+
+int64_t cko_check_tree(int scalar, int D, const void *tree, const int64_t *index,
+                       const int32_t *dims, int64_t n, const void *bounds, int nthreads)
+{
+  if (D < 1 || D > 8 || (dims && !bounds)) return -1;
+  check_ctx c = {scalar, D, (const float *)tree, (const int32_t *)tree, index, dims};
+  int64_t bad = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : bad) num_threads(nthreads)
+  for (int64_t i = 0; i < n; i++) {
+    /* ordering against every ancestor */
+    int64_t path[64];
+    int depth = 0;
+    for (int64_t child = i; child > 0;) {
+      const int64_t a = (child - 1) / 2;
+      const int r = composite_cmp(&c, i, a);
+      const int inLeft = child == 2 * a + 1;
+      if (inLeft ? r >= 0 : r <= 0) bad++;
+      path[depth++] = child;
+      child = a;
+    }
+    /* explicit dims: widest extent of the domain box */
+    if (dims) {
+      box_u box;
+      memcpy(box.f, bounds, sizeof(float) * 2 * D);
+      int64_t a = 0;
+      for (int l = depth - 1; l >= 0; l--) {
+        const int64_t child = path[l];
+        const int d = dims[a];
+        if (d < 0 || d >= D) {
+          bad++;
+          break;
+        }
+        if (scalar == 0) {
+          if (child == 2 * a + 1) box.f[D + d] = c.cf[a * D + d];
+          else box.f[d] = c.cf[a * D + d];
+        } else {
+          if (child == 2 * a + 1) box.i[D + d] = c.ci[a * D + d];
+          else box.i[d] = c.ci[a * D + d];
+        }
+        a = child;
+      }
+      const int want = scalar == 0 ? widest_f(box.f, box.f + D, D) : widest_i(box.i, box.i + D, D);
+      if (dims[i] != want) bad++;
+    }
+  }
+  return bad;
+}
+
+/* ===================================================================== */
 /* traversals                                                             */
 /* ===================================================================== */
 

@@ -39,6 +39,15 @@ enum { CKO_FIXED_LIST = 0, CKO_HEAP_LIST = 1 };
 int cko_build(int scalar, int D, const void *coords, int64_t n, int explicit_dim,
               int64_t *perm_out, int32_t *dims_out, void *bounds_out);
 
+/* Checks, without rebuilding, that `tree` ([n][D] coordinates in node order,
+ * index[node] = the point's input index) is the canonical tree cko_build
+ * returns: every node's left subtree below it and right subtree above it
+ * in the composite stable-sort key, and -- when dims is given -- every
+ * split dim the widest extent of the node's domain box inside `bounds`.
+ * Returns the number of violations (0 = canonical), -1 on bad arguments. */
+int64_t cko_check_tree(int scalar, int D, const void *tree, const int64_t *index,
+                       const int32_t *dims, int64_t n, const void *bounds, int nthreads);
+
 /* Number of nodes in the subtree under `node` of a left-balanced tree of n
  * nodes. */
 int64_t cko_subtree_size(int64_t node, int64_t n);

@@ -7,7 +7,10 @@ with the parameter vector laid out as
     W1[64][4], b1[64], W2[64][64] (W2[j][k]: output j, input k), b2[64],
     w3[64], b3.
 The GPU computes in FP32 over BF16-rounded weights; the oracle is given
-those same rounded weights, so the two differ only by FP32 rounding.
+those same rounded weights.  The inputs and the first hidden layer enter the
+GPU's products (tensor-core operands) as bf16, so the oracle rounds them the
+same way (round to nearest even of their FP32 value); what remains is FP32
+accumulation rounding.
 """
 import numpy as np
 
@@ -26,22 +29,35 @@ def unpack(p):
             p[OW3:OB3], p[OB3])
 
 
-def forward(p, f):
+def bf16(x):
+    """Round to the nearest bfloat16 (ties to even) through FP32."""
+    u = np.asarray(x, np.float64).astype(np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
+def forward(p, f, bf16_act=True):
+    """bf16_act: round the inputs and the first hidden layer as the GPU's
+    tensor-core operands are rounded (False: exact float64 network, for
+    checking the calculus by finite differences)."""
+    rnd = bf16 if bf16_act else (lambda x: np.asarray(x, np.float64))
     W1, b1, W2, b2, w3, b3 = unpack(p)
+    f = rnd(f)
     z1 = f @ W1.T + b1
-    h1 = np.maximum(z1, 0)
+    h1 = rnd(np.maximum(z1, 0))
     z2 = h1 @ W2.T + b2
     h2 = np.maximum(z2, 0)
     y = h2 @ w3 + b3
     return y, (h1, h2)
 
 
-def loss_and_grad(p, f, t):
-    """Mean squared error and its gradient w.r.t. the parameter vector."""
-    f = np.asarray(f, np.float64)
+def loss_and_grad(p, f, t, bf16_act=True):
+    """Mean squared error and its gradient w.r.t. the parameter vector (the
+    bf16 roundings pass gradients straight through, as on the GPU)."""
+    f = bf16(f) if bf16_act else np.asarray(f, np.float64)
     t = np.asarray(t, np.float64)
     W1, b1, W2, b2, w3, b3 = unpack(p)
-    y, (h1, h2) = forward(p, f)
+    y, (h1, h2) = forward(p, f, bf16_act)
     n = len(t)
     e = y - t
     loss = float(np.mean(e * e))

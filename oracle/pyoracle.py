@@ -56,6 +56,8 @@ def lib():
             subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
         L = C.CDLL(path)
         L.cko_build.argtypes = [C.c_int, C.c_int, _P, _I64, C.c_int, _P, _P, _P]
+        L.cko_check_tree.argtypes = [C.c_int, C.c_int, _P, _P, _P, _I64, _P, C.c_int]
+        L.cko_check_tree.restype = _I64
         L.cko_subtree_size.argtypes = [_I64, _I64]
         L.cko_subtree_size.restype = _I64
         L.cko_fcp.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _I64, _P, _P, _I64, C.c_float,
@@ -139,6 +141,23 @@ def build(coords, explicit_dim=False):
     if rc:
         raise RuntimeError(f"cko_build failed: {rc}")
     return perm, dims, bounds
+
+
+def check_tree(tree, index, dims=None, bounds=None, threads=None):
+    """Violations of the canonical-tree property (0 = the tree build()
+    returns for these points): tree [n, D] coordinates in node order,
+    index[node] = input index of the point there, dims per node for
+    explicit-dim trees (with the world bounds they were built in)."""
+    tree = np.ascontiguousarray(tree)
+    n, D = tree.shape
+    index = np.ascontiguousarray(index, np.int64)
+    d = None if dims is None else np.ascontiguousarray(dims, np.int32)
+    b = None if bounds is None else np.ascontiguousarray(bounds, dtype=tree.dtype)
+    r = lib().cko_check_tree(_scalar(tree), D, _ptr(tree), _ptr(index), _ptr(d), n, _ptr(b),
+                             threads or nthreads())
+    if r < 0:
+        raise ValueError("cko_check_tree: bad arguments")
+    return int(r)
 
 
 def subtree_size(node, n):

@@ -58,7 +58,7 @@ def test_training_reduces_loss_and_forward_matches_oracle():
     assert np.allclose(np.log(r), y * std + mean, rtol=0, atol=2e-3)
 
 
-@pytest.mark.parametrize("k", [8, 16, 32])
+@pytest.mark.parametrize("k", [2, 8, 16, 32])
 @pytest.mark.parametrize("method", ["stack_based", "stack_free", "cct"])
 def test_learned_results_identical_to_plain(k, method):
     n = 200000
@@ -90,6 +90,27 @@ def test_learned_radius_with_tiny_scale_falls_back_and_stays_exact():
     assert torch.equal(li, pi) and torch.equal(ld, pd)
 
 
+def test_learned_on_tie_heavy_tree_stays_exact():
+    """Points on a coarse integer lattice: whole groups of neighbours share
+    one squared distance, so the k-th boundary is tied for most queries;
+    every tied query must come back in the reference's own order."""
+    n = 60000
+    pts = wl.tie_heavy(n, levels=12, seed=4) * np.float32(0.05)
+    rec = torch.from_numpy(wl.packed_records(pts).view(np.int32).reshape(n, 4).copy()).cuda()
+    wb = ck.build_tree(rec, layout=LAYOUT)
+    m = ck.RadiusModel(seed=6)
+    m.fit(rec, torch.from_numpy(wl.uniform_points(20000, seed=13) * np.float32(0.55)).cuda(),
+          16, layout=LAYOUT, world_bounds=wb, epochs=2)
+    q = torch.from_numpy(wl.uniform_points(20000, seed=14) * np.float32(0.55)).cuda()
+    for method in ("stack_based", "stack_free", "cct"):
+        ri, rd = ck.knn(rec, q, 16, method, layout=LAYOUT, world_bounds=wb, reference_order=True)
+        for scale in (1.2, 3.0):
+            li, ld, fb, _ = ck.knn_learned(rec, q, 16, m, method, layout=LAYOUT,
+                                           world_bounds=wb, scale=scale)
+            assert torch.equal(li, ri)
+            assert np.array_equal(f32_bits(ld.cpu().numpy()), f32_bits(rd.cpu().numpy()))
+
+
 def test_trained_network_reduces_work():
     """What the trained network gains: every query the learned pass answers
     visits no more nodes than the plain search does (the radius only adds
@@ -117,3 +138,31 @@ def test_trained_network_reduces_work():
           f"learned {vl:.1f}  final loss {m.final_loss:.4f}")
     assert frac_fallback < 0.25
     assert vl < vp
+
+
+def test_trained_network_predicts_the_kth_distance():
+    """What training gives the range traversal: the trained network's radius
+    is close to each query's exact k-th distance (so the ball holds few
+    more than k points and few queries fall back), where the untrained
+    network's is not; both return the plain answers."""
+    n = 1000000
+    _, rec, wb = _tree(n)
+    q = torch.from_numpy(wl.mixed_queries(100000, seed=53)).cuda()
+    _, _, kth = ck.knn(rec, q, 16, layout=LAYOUT, world_bounds=wb, with_max=True)
+    true_r = torch.sqrt(kth)
+    untrained = ck.RadiusModel(grid_res=64, seed=4)
+    untrained.set_grid(rec, LAYOUT, wb)
+    trained = ck.RadiusModel(grid_res=64, seed=4)
+    trained.fit(rec, torch.from_numpy(wl.mixed_queries(200000, seed=51)).cuda(), 16,
+                layout=LAYOUT, world_bounds=wb, epochs=20, batch=4096)
+    ratio_t = (trained.predict(q) / true_r).log().abs()
+    ratio_u = (untrained.predict(q) / true_r).log().abs()
+    within_t = (ratio_t < np.log(1.25)).double().mean().item()
+    within_u = (ratio_u < np.log(1.25)).double().mean().item()
+    print(f"share of radii within 25% of the k-th distance: trained {within_t:.3f} "
+          f"untrained {within_u:.3f}")
+    assert within_t > 0.8 and within_u < 0.2
+    pi, pd = ck.knn(rec, q, 16, layout=LAYOUT, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(rec, q, 16, trained, layout=LAYOUT, world_bounds=wb)
+    assert torch.equal(li, pi) and torch.equal(ld, pd)
+    assert int(fb[0]) < 0.2 * q.shape[0]

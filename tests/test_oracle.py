@@ -219,10 +219,90 @@ def test_mlp_oracle_gradient_matches_finite_differences():
     p = rng.normal(0, 0.3, mo.NP)
     f = rng.normal(0, 1, (16, 4))
     t = rng.normal(0, 1, 16)
-    _, g = mo.loss_and_grad(p, f, t)
+    _, g = mo.loss_and_grad(p, f, t, bf16_act=False)
     for i in [0, 5, mo.OB1 + 3, mo.OW2 + 100, mo.OW2 + 4000, mo.OB2 + 7, mo.OW3 + 9, mo.OB3]:
         e = np.zeros(mo.NP)
         e[i] = 1e-6
-        lp, _ = mo.loss_and_grad(p + e, f, t)
-        lm, _ = mo.loss_and_grad(p - e, f, t)
+        lp, _ = mo.loss_and_grad(p + e, f, t, bf16_act=False)
+        lm, _ = mo.loss_and_grad(p - e, f, t, bf16_act=False)
         assert abs((lp - lm) / 2e-6 - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
+
+
+def test_mlp_oracle_bf16_rounding():
+    """The oracle's bf16 rounding (of the tensor-core operands) against
+    torch's bfloat16 conversion, ties included."""
+    import torch
+    from oracle import mlp_oracle as mo
+    rng = np.random.default_rng(1)
+    x = np.concatenate([rng.normal(0, 3, 4000), [0.0, 1.0, -2.5, 1.00390625, 1.01171875]])
+    x32 = x.astype(np.float32)
+    ref = torch.from_numpy(x32).to(torch.bfloat16).to(torch.float32).numpy()
+    assert np.array_equal(mo.bf16(x32).astype(np.float32), ref)
+
+
+# ---------------------------------------------------------------------------
+# the canonical-tree checker (used on trees too large to rebuild on the CPU)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("D", [2, 3, 4])
+@pytest.mark.parametrize("kind", ["uniform", "tie", "int"])
+@pytest.mark.parametrize("explicit", [False, True])
+def test_check_tree_accepts_oracle_builds(D, kind, explicit):
+    rng = np.random.Generator(np.random.MT19937(D * 7 + len(kind)))
+    n = 5003
+    if kind == "uniform":
+        pts = rng.random((n, D)).astype(np.float32)
+    elif kind == "tie":
+        pts = rng.integers(0, 4, size=(n, D)).astype(np.float32)
+    else:
+        pts = rng.integers(-50, 50, size=(n, D)).astype(np.int32)
+    perm, dims, bounds = po.build(pts, explicit_dim=explicit)
+    assert po.check_tree(pts[perm], perm, dims if explicit else None,
+                         bounds if explicit else None) == 0
+
+
+@pytest.mark.parametrize("explicit", [False, True])
+def test_check_tree_rejects_perturbed_trees(explicit):
+    rng = np.random.Generator(np.random.MT19937(3))
+    n = 3001
+    pts = rng.integers(0, 5, size=(n, 3)).astype(np.float32)  # many ties
+    perm, dims, bounds = po.build(pts, explicit_dim=explicit)
+    dm = dims if explicit else None
+    bd = bounds if explicit else None
+    tree, idx = pts[perm].copy(), perm.copy()
+    # two nodes whose points differ
+    i, j = 5, 2900
+    assert not np.array_equal(tree[i], tree[j])
+    t2, x2 = tree.copy(), idx.copy()
+    t2[[i, j]] = t2[[j, i]]
+    x2[[i, j]] = x2[[j, i]]
+    assert po.check_tree(t2, x2, dm, bd) > 0
+    # two nodes holding equal points: only the input-index tie-break differs
+    eq = [(a, b) for a in range(n) for b in range(a + 1, min(n, a + 400))
+          if np.array_equal(tree[a], tree[b]) and a != 0][:1]
+    a, b = eq[0]
+    x3 = idx.copy()
+    x3[[a, b]] = x3[[b, a]]
+    assert po.check_tree(tree, x3, dm, bd) > 0
+    if explicit:
+        d4 = dims.copy()
+        d4[17] = (d4[17] + 1) % 3
+        assert po.check_tree(tree, idx, d4, bounds) > 0
+
+
+@needs_ref
+@pytest.mark.parametrize("n", [1000, 40000])
+def test_check_tree_accepts_reference_host_builds(n):
+    """buildTree_host itself (unmodified reference code) passes the check,
+    explicit dims and ties included: the checker states the reference's
+    canonical order, not only this restatement's."""
+    rng = np.random.Generator(np.random.MT19937(n))
+    pts = rng.integers(0, 7, size=(n, 3)).astype(np.float32)
+    rec = np.zeros(n, po.ref_record_dtype(po.REF_F3_PACKED))
+    rec["p"] = pts
+    rec["payload"] = np.arange(n, dtype=np.uint32)
+    out, rb = po.ref_build_host(po.REF_F3_PACKED, rec)
+    idx = (out["payload"] & 0x3FFFFFFF).astype(np.int64)
+    dims = (out["payload"] >> 30).astype(np.int32)
+    assert po.check_tree(np.ascontiguousarray(out["p"]), idx, dims, rb) == 0
+    out2, _ = po.ref_build_host(po.REF_F3_PAYLOAD, rec.view(po.ref_record_dtype(po.REF_F3_PAYLOAD)))
+    assert po.check_tree(np.ascontiguousarray(out2["p"]), out2["payload"].astype(np.int64)) == 0
