@@ -36,6 +36,7 @@ N_QUERIES = 10_000_000
 K = 16
 RECORD_BYTES = 16
 METRIC = "knn_queries_per_s"
+PARITY_SAMPLE = 1_000_000
 UNIT = "queries/s"
 
 
@@ -51,6 +52,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the C1 / C4 / C5 measurements of the default line")
     ap.add_argument("--batched-clouds", type=int, default=4096,
                     help="clouds in the batched section (4096 = the configuration)")
     ap.add_argument("--batched-tuning", default="",
@@ -76,6 +79,15 @@ def workload_desc(n, nq):
         return f"{x / 1e6:g}M" if x >= 1e6 else str(x)
     return (f"build (widest-dim, 16-byte {{float3,payload+dim}} records) + kNN k={K} "
             f"stack-based over {m(n)} Gaussian-mixture points and {m(nq)} mixture queries")
+
+
+def bench_config(n, nq, world):
+    """The workload description both arms print (same keys, same values)."""
+    return {"workload": workload_desc(n, nq), "points": n, "queries": nq, "k": K,
+            "record_bytes": RECORD_BYTES, "split": "widest extent (explicit dim)",
+            "traversal": "stack_based", "morton_reorder": True,
+            "l2": "inputs exceed L2 (160 MB points + 120 MB queries), no flush",
+            "parallelism": f"replicas x{world}"}
 
 
 def workload(n_points, n_queries):
@@ -234,6 +246,10 @@ def run_ours(args, rank, world, local):
     t_ms = max_over_ranks(e0.elapsed_time(e1), pg, dev)
     ms_per_step = t_ms / args.steps
     value = whole_job_rate(nq, world, ms_per_step)
+    # the last step's answers for the first PARITY_SAMPLE queries: checked
+    # against the reference's host traversal in the CPU-baseline leg
+    ns = min(nq, PARITY_SAMPLE)
+    step_out = (d_ids[:ns].cpu().numpy(), d_d2[:ns].cpu().numpy())
 
     # ---- phase timings (same stream, CUDA events), outside the timed region
     def timed(fn, reps=3):
@@ -262,11 +278,20 @@ def run_ours(args, rank, world, local):
                                       world_bounds=wb, out_ids=d_ids, out_d2=d_d2,
                                       reference_order=True), reps=1)
     morton_ms = timed(lambda: ck.morton_order(d_q))
+    # the traversal kernel without the reorder: the same queries already in
+    # Morton order (cukd_knn then runs knn_fast_kernel and the re-run of the
+    # few tied queries)
+    d_qs = d_q[ck.morton_order(d_q).long()].contiguous()
+    knn_kernel_ms = timed(lambda: ck.knn(d_pts, d_qs, K, "stack_based", layout=lay,
+                                         world_bounds=wb, out_ids=d_ids, out_d2=d_d2,
+                                         morton=False))
+    del d_qs
     fcp_ms = timed(lambda: ck.fcp(d_pts, d_q, "stack_based", layout=lay, world_bounds=wb))
 
     # ---- learned radius vs plain on the same queries (config 4's method on
     # this workload: trained on 1M queries from the query distribution)
     learned = None
+    learned_out = None
     if not args.no_learned:
         from cudakdtree_b200 import workloads as wl
         ntrain = min(1_000_000, nq)
@@ -284,10 +309,14 @@ def run_ours(args, rank, world, local):
                                    world_bounds=wb, scale=1.2, out_ids=d_ids, out_d2=d_d2)[2]
 
         learned_ms = timed(run_learned)
+        learned_out = (d_ids[:ns].cpu().numpy(), d_d2[:ns].cpu().numpy())
         learned = {"knn_ms": round(learned_ms, 3), "plain_knn_ms": round(knn_sb_ms, 3),
                    "speedup_vs_plain": round(knn_sb_ms / learned_ms, 3),
-                   "reference_order_knn_ms": round(knn_ref_ms, 3),
-                   "speedup_vs_reference_order": round(knn_ref_ms / learned_ms, 3),
+                   "target_speedup_vs_plain": 1.5,
+                   "target_met": bool(knn_sb_ms / learned_ms >= 1.5),
+                   "path": ("cukd_knn_learned: Morton order, knn_learned_kernel (MLP on the "
+                            "tensor cores fused with the seeded traversal), plain re-run of "
+                            "the fallbacks, reference-order re-run of ties"),
                    "queries_per_s": round(nq / (learned_ms / 1e3), 1),
                    "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
                    "reference_order_reruns": int(fb[0][1].item()),
@@ -299,11 +328,16 @@ def run_ours(args, rank, world, local):
     visits = ck.knn_visits(d_pts, d_q, K, "stack_based", layout=lay, world_bounds=wb)
     tot_visits = int(visits.sum().item())
     knn_bytes = tot_visits * RECORD_BYTES + nq * 12 + nq * K * 8
-    achieved = knn_bytes / (knn_sb_ms / 1e3) / 1e9
+    achieved = knn_bytes / (knn_kernel_ms / 1e3) / 1e9
     traffic = profile_traffic("knn_stack_based_k16_10M")
-    roofline = {"bound": "hbm", "kernel": "knn stack-based k=16 (cukd_knn: Morton order + "
-                "knn_fast_kernel + reference-order re-run of tied queries)", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": "knn_fast_kernel, stack-based k=16",
+                "timed": ("cukd_knn on the queries already in Morton order, CUDA events on "
+                          "the launching stream: knn_fast_kernel plus the re-run of the few "
+                          "tied queries"),
+                "kernel_ms": round(knn_kernel_ms, 3),
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
+                "frac_of_whole_knn_call": round(knn_bytes / (knn_sb_ms / 1e3) / 1e9 / peak, 4),
                 "algorithmic_bytes": knn_bytes,
                 "bytes_formula": "sum(visits_ref)*16 + nq*12 + nq*k*8",
                 "mean_visits_per_query": round(tot_visits / nq, 2), "peak_source": peak_src}
@@ -392,28 +426,43 @@ def run_ours(args, rank, world, local):
     batched = None if args.no_batched else batched_section(ck, dev, args.batched_clouds,
                                                            args.batched_tuning)
 
+    others = None
+    if world == 1 and not args.no_configs:
+        # the other configurations, each measured once (parity-test workloads
+        # of the full suite): freed of this workload's buffers first
+        keep_pts = d_pts.cpu().numpy() if rank == 0 and not args.no_cpu_baseline else None
+        keep_wb = wb.cpu().numpy()
+        del d_src, d_pts, d_q, d_ids, d_d2
+        torch.cuda.empty_cache()
+        others = {}
+        for name, fn in (("c1", config_c1), ("c4", config_c4), ("c5", config_c5)):
+            others[name] = fn(ck, dev, peak)
+            torch.cuda.empty_cache()
+    else:
+        keep_pts = d_pts.cpu().numpy() if rank == 0 and not args.no_cpu_baseline else None
+        keep_wb = wb.cpu().numpy()
+
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(d_pts.cpu().numpy(), wb.cpu().numpy(), q)
+        cpu = cpu_baseline_sample(keep_pts, keep_wb, q, step_out, learned_out)
+        parity = cpu.pop("parity", None)
 
     out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded Gaussian mixture, 64 components, sigma 0.01)",
-           "config": {"workload": workload_desc(n, nq), "points": n, "queries": nq, "k": K,
-                      "record_bytes": RECORD_BYTES, "split": "widest extent (explicit dim)",
-                      "traversal": "stack_based", "morton_reorder": True,
-                      "l2": "inputs exceed L2 (160 MB points + 120 MB queries), no flush",
-                      "parallelism": f"replicas x{world}"},
+           "config": bench_config(n, nq, world),
            "phases_ms": {"build": round(build_ms, 3), "knn_stack_based": round(knn_sb_ms, 3),
                          "knn_stack_free": round(knn_sf_ms, 3), "morton_order": round(morton_ms, 3),
                          "fcp_stack_based": round(fcp_ms, 3), "restore_copy": round(copy_ms, 3),
                          "knn_stack_based_reference_order": round(knn_ref_ms, 3)},
            "build_ms": round(build_ms, 3),
            "knn_stack_free_queries_per_s": round(nq / (knn_sf_ms / 1e3), 1),
-           "learned_radius": learned, "batched": batched,
+           "learned_radius": learned, "batched": batched, "other_configs": others,
            "roofline": roofline, "build_roofline": build_roof,
-           "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
+           "cpu_baseline": cpu, "parity": parity,
+           "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
            "gpu_launches_per_step": round(launches / args.steps, 1)}
     if pg:
         pg.destroy_process_group()
@@ -479,9 +528,13 @@ def batched_section(ck, dev, num_clouds=4096, tuning=""):
             "kernel_launches_per_run": launches, "graph": True}
 
 
-def cpu_baseline_sample(tree_records_i32, bounds, q):
+def cpu_baseline_sample(tree_records_i32, bounds, q, step_out, learned_out=None):
     """The reference's own host code (oracle/_ref) on a bounded sample of
-    the workload, on this box's host cores."""
+    the workload, on this box's host cores; on the same sample, the parity
+    check of this run's answers: the reference's host traversal must return
+    the step's kNN ids and squared-distance bits (and the learned path's),
+    and the GPU-built tree must be the reference's canonical tree (the
+    oracle's canonical-tree checker, pinned to buildTree_host in the tests)."""
     try:
         from oracle import pyoracle as po
         if po.ref_host() is None:
@@ -489,11 +542,33 @@ def cpu_baseline_sample(tree_records_i32, bounds, q):
         from cudakdtree_b200 import workloads as wl
         cores = po.nthreads()
         rec = tree_records_i32.view(po.ref_record_dtype(po.REF_F3_PACKED)).reshape(-1)
-        ns = min(len(q), 1_000_000)
+        step_ids, step_d2 = step_out
+        ns = len(step_ids)
         qs = np.ascontiguousarray(q[:ns])
         t = time.perf_counter()
-        po.ref_knn_host(po.REF_F3_PACKED, rec, bounds, qs, K, po.STACK_BASED, threads=cores)
+        ri, rd, _ = po.ref_knn_host(po.REF_F3_PACKED, rec, bounds, qs, K, po.STACK_BASED,
+                                    threads=cores)
         tq = time.perf_counter() - t
+
+        def same(out):
+            return bool(np.array_equal(out[0], ri) and
+                        np.array_equal(np.ascontiguousarray(out[1]).view(np.uint32),
+                                       rd.view(np.uint32)))
+        pay = tree_records_i32[:, 3].view(np.uint32)
+        perm = (pay & 0x3FFFFFFF).astype(np.int64)
+        dims = (pay >> 30).astype(np.int32)
+        coords = np.ascontiguousarray(tree_records_i32[:, :3]).view(np.float32)
+        is_perm = bool(np.array_equal(np.sort(perm), np.arange(len(perm))))
+        violations = po.check_tree(coords, perm, dims, bounds) if is_perm else -1
+        parity = {"sample_queries": ns, "knn_equal_reference": same(step_out),
+                  "tree_canonical": bool(violations == 0),
+                  "checker": ("reference stackBased::knn host traversal (oracle/_ref) on the "
+                              "GPU-built tree; canonical-tree check of the whole tree")}
+        if learned_out is not None:
+            parity["learned_equal_reference"] = same(learned_out)
+        parity["ok"] = all(v for key, v in parity.items()
+                           if key in ("knn_equal_reference", "tree_canonical",
+                                      "learned_equal_reference"))
         nb = 1_000_000
         sub = wl.packed_records(wl.gmm_points(nb, seed=3))
         sub_rec = sub.view(po.ref_record_dtype(po.REF_F3_PACKED))
@@ -503,18 +578,24 @@ def cpu_baseline_sample(tree_records_i32, bounds, q):
         return {"value": round(ns / tq, 1), "unit": UNIT, "cores": cores, "kind": "reference",
                 "sample": (f"reference stackBased::knn<FixedCandidateList<16>> (OpenMP, {cores} "
                            f"threads) on {ns} of the 10M queries against the full 10M-point tree "
-                           "(query phase only; the tree is the GPU build, byte-identical to "
-                           "buildTree_host's); reference buildTree_host on a 1M-point sample of "
-                           f"the mixture took {tb:.2f} s single-threaded"),
-                "build_1M_sample_s": round(tb, 3)}
+                           "(query phase only; the tree is the GPU build, checked canonical); "
+                           "reference buildTree_host on a 1M-point sample of the mixture took "
+                           f"{tb:.2f} s single-threaded"),
+                "build_1M_sample_s": round(tb, 3), "parity": parity}
     except Exception as e:  # the baseline is reported, never required
-        return {"value": None, "unit": UNIT, "unavailable": repr(e)[:200]}
+        return {"value": None, "unit": UNIT, "unavailable": repr(e)[:200],
+                "parity": {"ok": False, "error": repr(e)[:200]}}
 
 
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU implementation of the path
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world, local):
+    """The reference's own CPU code (oracle/_ref, compiled unmodified) on
+    this arm's workload: cukd::buildTree_host over all points, timed once
+    (single-threaded as the reference implements it, 48 s at 10M), then every
+    step answers all the queries with stackBased::knn<FixedCandidateList<16>>
+    in an OpenMP loop over every host thread (sampleHost.cu:58-73)."""
     if rank != 0:
         return
     from oracle import pyoracle as po
@@ -528,32 +609,29 @@ def run_reference(args, rank, world, local):
     t = time.perf_counter()
     tree, bounds = po.ref_build_host(po.REF_F3_PACKED, rec)
     t_build = time.perf_counter() - t
-    sample = min(nq, 1_000_000)
+    qs = np.ascontiguousarray(q)
 
-    def knn_sample(i):
-        lo = (i * sample) % max(1, nq - sample + 1)
-        qs = np.ascontiguousarray(q[lo:lo + sample])
+    def knn_step():
         t0 = time.perf_counter()
         po.ref_knn_host(po.REF_F3_PACKED, tree, bounds, qs, K, po.STACK_BASED, threads=cores)
         return time.perf_counter() - t0
 
-    for i in range(args.warmup):
-        knn_sample(i)
-    times = [knn_sample(args.warmup + i) for i in range(args.steps)]
-    t_knn = float(np.mean(times)) * (nq / sample)
-    step_s = t_build + t_knn
+    for _ in range(args.warmup):
+        knn_step()
+    times = [knn_step() for _ in range(args.steps)]
+    step_s = float(np.mean(times))
     value = nq / step_s
-    desc = (f"cukd::buildTree_host (single-threaded, as the reference implements it) on all "
-            f"{n} points timed once ({t_build:.2f} s) + stackBased::knn<FixedCandidateList<16>> "
-            f"on {sample}-query samples per step with {cores} OpenMP threads, scaled to {nq} "
-            "queries")
+    desc = (f"every step: stackBased::knn<FixedCandidateList<16>> over all {nq} queries with "
+            f"{cores} OpenMP threads against the {n}-point tree; cukd::buildTree_host "
+            f"(single-threaded, as the reference implements it) timed once: {t_build:.2f} s, "
+            "reported as build_ms and not repeated per step")
     ref_gpu = reference_gpu_timings(recs, q)
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (same seeds as our arm)",
-           "config": {"workload": workload_desc(n, nq), "points": n, "queries": nq, "k": K,
-                      "parallelism": "host cores"},
+           "config": bench_config(n, nq, world),
+           "reference_step": desc,
            "build_ms": round(t_build * 1e3, 1),
            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores,
                             "kind": "reference", "sample": desc},
@@ -646,7 +724,20 @@ def _timer():
     return timed
 
 
-def config_c1(ck, dev):
+def _frac(bytes_, ms, peak):
+    return round(bytes_ / (ms / 1e3) / 1e9 / peak, 4)
+
+
+def _knn_bytes(ck, tree, q, k, rec_bytes, qbytes, scale=1, **kw):
+    """Algorithmic bytes of a kNN launch: every node the reference's
+    stack-based traversal visits read once, the queries read, (id, d2)
+    written -- visits counted on `q` (a sample), scaled by `scale`."""
+    v = int(ck.knn_visits(tree, q, k, "stack_based", **kw).sum().item()) * scale
+    nq = q.shape[0] * scale
+    return v * rec_bytes + nq * qbytes + nq * k * 8, v / nq
+
+
+def config_c1(ck, dev, peak):
     """1M U[0,1)^3 float3 points (seed 1), 1M U[0,1)^3 queries (seed 2),
     round-robin dims; FCP and kNN k=8 with the three traversals; the
     reference's host build + host traversals on the same data for context."""
@@ -661,14 +752,24 @@ def config_c1(ck, dev):
     lay = ck.layout_for("float32", 3)
     wb = torch.empty((2, 3), dtype=torch.float32, device=dev)
     copy = lambda: P.copy_(src)
+    sampler = ClockSampler(dev.index or 0)
+    sampler.start()
     build_ms = timed(lambda: ck.build_tree(P, layout=lay, world_bounds=wb), reps=5, setup=copy)
+    n = len(pts)
     out = {"config": "C1", "workload": "1M uniform float3, 1M uniform queries, round-robin",
-           "build_ms": round(build_ms, 3), "queries_per_s": {}}
+           "build_ms": round(build_ms, 3),
+           "build_frac": _frac(2 * n * 12 * (int(np.log2(n)) + 1), build_ms, peak),
+           "queries_per_s": {}}
     for m in ("stack_based", "stack_free", "cct"):
         t = timed(lambda: ck.fcp(P, Q, m, layout=lay, world_bounds=wb))
         out["queries_per_s"][f"fcp_{m}"] = round(len(q) / (t / 1e3), 1)
         t = timed(lambda: ck.knn(P, Q, 8, m, layout=lay, world_bounds=wb))
         out["queries_per_s"][f"knn8_{m}"] = round(len(q) / (t / 1e3), 1)
+        if m == "stack_based":
+            kb, mv = _knn_bytes(ck, P, Q, 8, 12, 12, layout=lay, world_bounds=wb)
+            out["knn8_frac"] = _frac(kb, t, peak)
+            out["knn8_mean_visits_ref"] = round(mv, 2)
+    out["clocks"] = sampler.stop()
     try:
         from oracle import pyoracle as po
         if po.ref_host() is not None:
@@ -691,7 +792,7 @@ def config_c1(ck, dev):
     return out
 
 
-def config_c2(ck, dev):
+def config_c2(ck, dev, peak=None):
     """The benchmark workload's data with every builder name, the spatial
     tree, and kNN k=16 with the three traversals."""
     import torch
@@ -730,7 +831,7 @@ def config_c2(ck, dev):
     return out
 
 
-def config_c4(ck, dev):
+def config_c4(ck, dev, peak):
     """Learned radius at k = 32: model trained on 1M queries of the serving
     distribution (70% mixture / 30% uniform, their own seed), then 50M such
     queries answered plain and learned."""
@@ -755,6 +856,8 @@ def config_c4(ck, dev):
     Q = torch.from_numpy(wl.mixed_queries(nq)).to(dev)
     ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
     d2 = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    sampler = ClockSampler(dev.index or 0)
+    sampler.start()
     t_plain = timed(lambda: ck.knn(P, Q, k, "stack_based", layout=lay, world_bounds=wb,
                                    out_ids=ids, out_d2=d2), reps=2)
     ref_ids = ids.clone()
@@ -764,41 +867,52 @@ def config_c4(ck, dev):
         fb[0] = ck.knn_learned(P, Q, k, model, "stack_based", layout=lay, world_bounds=wb,
                                scale=1.2, out_ids=ids, out_d2=d2)[2]
     t_learned = timed(learned, reps=2)
+    clocks = sampler.stop()
     same = bool(torch.equal(ids, ref_ids))
-    t_ref = timed(lambda: ck.knn(P, Q[:5_000_000], k, "stack_based", layout=lay,
-                                 world_bounds=wb, reference_order=True), reps=1) * 10
+    kb, mv = _knn_bytes(ck, P, Q[:5_000_000], k, RECORD_BYTES, 12, scale=10, layout=lay,
+                        world_bounds=wb)
     return {"config": "C4", "workload": "10M-point mixture tree, k=32, train on 1M and infer "
             "50M queries (70% mixture / 30% uniform), radius x1.2",
             "train_s": round(train_s, 3), "final_loss": round(model.final_loss, 5),
-            "plain_fast_ms": round(t_plain, 3), "learned_ms": round(t_learned, 3),
-            "reference_order_ms_est": round(t_ref, 1),
-            "speedup_vs_plain_fast": round(t_plain / t_learned, 3),
-            "speedup_vs_reference_order": round(t_ref / t_learned, 3),
+            "plain_knn_ms": round(t_plain, 3), "learned_knn_ms": round(t_learned, 3),
+            "plain_queries_per_s": round(nq / (t_plain / 1e3), 1),
+            "learned_queries_per_s": round(nq / (t_learned / 1e3), 1),
+            "learned_speedup_vs_plain": round(t_plain / t_learned, 3),
+            "plain_knn_frac": _frac(kb, t_plain, peak),
             "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
-            "identical_results": same}
+            "identical_results": same, "clocks": clocks}
 
 
-def config_c5(ck, dev):
-    """100M float4 points (xyz U[0,1), w N(0,1)) with widest-extent dims in a
-    {float4; int dim} record, and 20M int3 points in [-2^20, 2^20]^3 with
-    round-robin dims; kNN k = 64 on 20M queries of each distribution."""
+# the reference's {float4 p; int dim;} record: 32 bytes (float4 is 16-byte
+# aligned)
+F4_STRIDE = 32
+
+
+def config_c5(ck, dev, peak):
+    """100M float4 points (xyz U[0,1), w N(0,1)) with widest-extent dims in
+    the reference's 32-byte {float4; int dim} record, and 20M int3 points in
+    [-2^20, 2^20]^3 with round-robin dims; kNN k = 64 on 20M queries of each
+    distribution."""
     import torch
     from cudakdtree_b200 import workloads as wl
     timed = _timer()
     out = {"config": "C5"}
     n, nq, k = 100_000_000, 20_000_000, 64
     p4 = wl.wide_float4(n, seed=7)
-    rec = np.zeros((n, 5), np.float32)
+    rec = np.zeros((n, F4_STRIDE // 4), np.float32)
     rec[:, :4] = p4
     del p4
-    lay = ck.layout_for("float32", 4, stride=20, dim_offset=16)
+    lay = ck.layout_for("float32", 4, stride=F4_STRIDE, dim_offset=16)
     src = torch.from_numpy(rec.view(np.uint8).reshape(-1)).to(dev)
     del rec
     P = torch.empty_like(src)
     wb = torch.empty((2, 4), dtype=torch.float32, device=dev)
-    out["float4_100M_build_ms"] = round(timed(lambda: ck.build_tree(P, layout=lay, world_bounds=wb,
-                                                                    n=n),
-                                              setup=lambda: P.copy_(src), reps=2), 3)
+    sampler = ClockSampler(dev.index or 0)
+    sampler.start()
+    bms = timed(lambda: ck.build_tree(P, layout=lay, world_bounds=wb, n=n),
+                setup=lambda: P.copy_(src), reps=2)
+    out["float4_100M_build_ms"] = round(bms, 3)
+    out["float4_build_frac"] = _frac(2 * n * F4_STRIDE * (int(np.log2(n)) + 1), bms, peak)
     del src
     Q = torch.from_numpy(wl.wide_float4(nq, seed=9)).to(dev)
     ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
@@ -806,6 +920,9 @@ def config_c5(ck, dev):
     t = timed(lambda: ck.knn(P, Q, k, "stack_based", layout=lay, world_bounds=wb, n=n,
                              out_ids=ids, out_d2=d2), reps=1)
     out["float4_knn64_queries_per_s"] = round(nq / (t / 1e3), 1)
+    kb, mv = _knn_bytes(ck, P, Q[:1_000_000], k, F4_STRIDE, 16, scale=nq // 1_000_000,
+                        layout=lay, world_bounds=wb, n=n)
+    out["float4_knn64_frac"] = _frac(kb, t, peak)
     out["float4_learned"] = "unavailable: the learned radius model is float3-only"
     del P, Q, ids, d2
     torch.cuda.empty_cache()
@@ -815,12 +932,18 @@ def config_c5(ck, dev):
     Pi = torch.empty_like(srci)
     layi = ck.layout_for("int32", 3)
     wbi = torch.empty((2, 3), dtype=torch.int32, device=dev)
-    out["int3_20M_build_ms"] = round(timed(lambda: ck.build_tree(Pi, layout=layi, world_bounds=wbi),
-                                           setup=lambda: Pi.copy_(srci), reps=2), 3)
+    bms = timed(lambda: ck.build_tree(Pi, layout=layi, world_bounds=wbi),
+                setup=lambda: Pi.copy_(srci), reps=2)
+    out["int3_20M_build_ms"] = round(bms, 3)
+    out["int3_build_frac"] = _frac(2 * len(pi) * 12 * (int(np.log2(len(pi))) + 1), bms, peak)
     Qi = torch.from_numpy(qi).to(dev)
     t = timed(lambda: ck.knn(Pi, Qi, k, "stack_based", layout=layi, world_bounds=wbi), reps=1)
     out["int3_knn64_queries_per_s"] = round(nq / (t / 1e3), 1)
+    kb, mv = _knn_bytes(ck, Pi, Qi[:1_000_000], k, 12, 12, scale=nq // 1_000_000, layout=layi,
+                        world_bounds=wbi)
+    out["int3_knn64_frac"] = _frac(kb, t, peak)
     out["int3_learned"] = "unavailable: the learned radius model is float3-only"
+    out["clocks"] = sampler.stop()
     try:
         from oracle import pyoracle as po
         tree = Pi.cpu().numpy()
@@ -841,8 +964,9 @@ def run_configs(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     fns = {"c1": config_c1, "c2": config_c2, "c4": config_c4, "c5": config_c5}
+    peak, _ = measured_peaks()
     for name in [c.strip().lower() for c in args.configs.split(",") if c.strip()]:
-        res = fns[name](ck, dev)
+        res = fns[name](ck, dev, peak)
         print(json.dumps(res), flush=True)
         torch.cuda.empty_cache()
 

@@ -76,3 +76,8 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert out["impl"] == "reference" and out["n_gpus"] == 2
     assert out["value"] > 0 and out["e2e"]["h2d_bytes_per_step"] == 0
     assert out["cpu_baseline"]["kind"] == "reference"
+    # the arm describes its workload with exactly the product arm's config
+    import bench
+    assert out["config"] == bench.bench_config(3000, 2000, 2)
+    # every step answers all the queries; the build is reported once
+    assert out["build_ms"] > 0 and "all 2000 queries" in out["reference_step"]
