@@ -37,6 +37,10 @@ K = 16
 RECORD_BYTES = 16
 METRIC = "knn_queries_per_s"
 PARITY_SAMPLE = 1_000_000
+# the learned radius network's training loss: pinball at this quantile of the
+# k-th distance (fewer fallbacks than the mean-squared-error fit at the same
+# radius scale, measured on the 10M-point benchmark and on config 4)
+LEARNED_QUANTILE = 0.9
 UNIT = "queries/s"
 
 
@@ -54,6 +58,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the C1 / C4 / C5 measurements of the default line")
+    ap.add_argument("--kernel-case", default="", choices=[""] + sorted(KERNEL_CASES),
+                    help="run one small single-kernel case twice (the workloads of the "
+                         "per-kernel ncu captures summarised under profiles/) and exit")
     ap.add_argument("--batched-clouds", type=int, default=4096,
                     help="clouds in the batched section (4096 = the configuration)")
     ap.add_argument("--batched-tuning", default="",
@@ -296,7 +303,7 @@ def run_ours(args, rank, world, local):
         from cudakdtree_b200 import workloads as wl
         ntrain = min(1_000_000, nq)
         qtrain = torch.from_numpy(wl.gmm_points(ntrain, seed=3, sample_seed=14)).to(dev)
-        model = ck.RadiusModel(grid_res=64, seed=1)
+        model = ck.RadiusModel(grid_res=64, seed=1, quantile=LEARNED_QUANTILE)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         model.fit(d_pts, qtrain, K, layout=lay, world_bounds=wb, epochs=10, batch=4096)
@@ -321,6 +328,7 @@ def run_ours(args, rank, world, local):
                    "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
                    "reference_order_reruns": int(fb[0][1].item()),
                    "train_s": round(train_s, 3), "train_queries": ntrain,
+                   "training_loss": f"pinball at quantile {LEARNED_QUANTILE}",
                    "final_loss": round(model.final_loss, 5), "radius_scale": 1.2}
 
     # ---- roofline of the dominant kernel (kNN traversal)
@@ -846,7 +854,7 @@ def config_c4(ck, dev, peak):
     wb = ck.build_tree(P, layout=lay)
     k = 32
     qtrain = torch.from_numpy(wl.mixed_queries(1_000_000, seed=14)).to(dev)
-    model = ck.RadiusModel(grid_res=64, seed=1)
+    model = ck.RadiusModel(grid_res=64, seed=1, quantile=LEARNED_QUANTILE)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     model.fit(P, qtrain, k, layout=lay, world_bounds=wb, epochs=10, batch=4096)
@@ -958,6 +966,89 @@ def config_c5(ck, dev, peak):
     return out
 
 
+# ---------------------------------------------------------------------------
+# small single-kernel cases (per-kernel ncu captures): inputs above the L2
+# size, a few GB on the device at most; each runs its kernel(s) twice
+# ---------------------------------------------------------------------------
+def _gmm_tree(ck, n=10_000_000):
+    import torch
+    from cudakdtree_b200 import workloads as wl
+    lay = ck.layout_for("float32", 3, stride=16, dim_offset=12, dim_shift=30, dim_bits=2)
+    rec = torch.from_numpy(wl.packed_records(wl.gmm_points(n, seed=3)).view(np.int32)
+                           .reshape(n, 4).copy()).cuda()
+    return rec, ck.build_tree(rec, layout=lay), lay
+
+
+def kernel_case(name):
+    import torch
+    import cudakdtree_b200 as ck
+    from cudakdtree_b200 import workloads as wl
+
+    def gmm_q(nq):
+        return torch.from_numpy(wl.gmm_points(nq, seed=3, sample_seed=4)).cuda()
+    if name == "knn":  # knn_fast_kernel: 10M-point tree, 2M queries, k = 16
+        rec, wb, lay = _gmm_tree(ck)
+        q = gmm_q(2_000_000)
+        for _ in range(2):
+            ck.knn(rec, q, 16, "stack_based", layout=lay, world_bounds=wb)
+    elif name in ("learned", "train", "infer"):
+        rec, wb, lay = _gmm_tree(ck)
+        q = gmm_q(2_000_000)
+        m = ck.RadiusModel(grid_res=64, seed=1, quantile=LEARNED_QUANTILE)
+        m.fit(rec, torch.from_numpy(wl.gmm_points(1_000_000, seed=3, sample_seed=14)).cuda(),
+              16, layout=lay, world_bounds=wb, epochs=2, batch=4096)
+        for _ in range(2):
+            if name == "infer":
+                m.predict(q)
+            else:
+                ck.knn_learned(rec, q, 16, m, "stack_based", layout=lay, world_bounds=wb,
+                               scale=1.2)
+    elif name == "heap":  # k = 64: knn_fast_heap_kernel
+        rec, wb, lay = _gmm_tree(ck)
+        q = gmm_q(1_000_000)
+        for _ in range(2):
+            ck.knn(rec, q, 64, "stack_based", layout=lay, world_bounds=wb)
+    elif name == "fastint":  # 20M int3 points, k = 64
+        p = torch.from_numpy(wl.int3_points(20_000_000)).cuda()
+        wb = ck.build_tree(p)
+        q = torch.from_numpy(wl.int3_points(1_000_000, seed=9)).cuda()
+        for _ in range(2):
+            ck.knn(p, q, 64, world_bounds=wb)
+    elif name == "accumulate":  # sharded kNN fold: two 2M-point shards
+        from cudakdtree_b200 import shard
+        pts = wl.gmm_points(4_000_000, seed=3)
+        for _ in range(2):
+            shard.sharded_knn([torch.from_numpy(pts[:2_000_000]).cuda(),
+                               torch.from_numpy(pts[2_000_000:]).cuda()], 16)
+    elif name == "spatial":  # spatial tree over 10M points, kNN k = 16 (cct)
+        pts = torch.from_numpy(wl.gmm_points(10_000_000, seed=3)).cuda()
+        q = gmm_q(2_000_000)
+        t = None
+        for _ in range(2):
+            if t is not None:
+                t.free()
+            t = ck.spatial_build(pts)
+            t.knn(q, 16, "cct")
+    elif name == "scatter":  # Morton order of 10M queries
+        q = torch.from_numpy(wl.gmm_points(10_000_000, seed=3, sample_seed=4)).cuda()
+        for _ in range(2):
+            ck.morton_order(q)
+    elif name == "build":  # the benchmark's 10M-point build
+        lay = ck.layout_for("float32", 3, stride=16, dim_offset=12, dim_shift=30, dim_bits=2)
+        src = torch.from_numpy(wl.packed_records(wl.gmm_points(10_000_000, seed=3))
+                               .view(np.int32).reshape(-1, 4).copy()).cuda()
+        d = torch.empty_like(src)
+        for _ in range(2):
+            d.copy_(src)
+            ck.build_tree(d, layout=lay)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": name, "ok": True}))
+
+
+KERNEL_CASES = ("knn", "learned", "train", "infer", "heap", "fastint", "accumulate", "spatial",
+                "scatter", "build")
+
+
 def run_configs(args):
     import torch
     import cudakdtree_b200 as ck
@@ -974,6 +1065,9 @@ def run_configs(args):
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.kernel_case:
+        kernel_case(args.kernel_case)
+        return
     if args.configs:
         if rank == 0:
             run_configs(args)

@@ -44,6 +44,7 @@ BUILDERS = {"default": 0, "thrust": 1, "bitonic": 2, "inplace": 3, "inPlace": 3}
 QUERY_MORTON, QUERY_HEAP_ORDER, QUERY_FORCE_HEAP, QUERY_REFERENCE_ORDER = 1, 2, 4, 8
 QUERY_TREE_ORDER = 16
 INT64_MAX = (1 << 63) - 1
+ASYNC_WAIT_POLLS_DEFAULT = 4194304  # CUKD_ASYNC_WAIT_POLLS_DEFAULT
 
 
 class CukdError(RuntimeError):
@@ -171,6 +172,9 @@ def lib():
         L.cukd_status_string.restype = C.c_char_p
         L.cukd_last_cuda_error.restype = C.c_char_p
         L.cukd_launch_count.restype = C.c_ulonglong
+        L.cukd_build_check.argtypes = [P]
+        L.cukd_set_async_wait_polls.argtypes = [C.c_uint32]
+        L.cukd_async_wait_timeouts.argtypes = [C.POINTER(C.c_uint)]
         L.cukd_spatial_build.argtypes = [P, I64, C.POINTER(Layout), C.c_int,
                                          C.POINTER(SpatialTreeC), P, C.POINTER(MemResource)]
         L.cukd_spatial_free.argtypes = [C.POINTER(SpatialTreeC), P, C.POINTER(MemResource)]
@@ -180,6 +184,7 @@ def lib():
                                        C.POINTER(QueryParams), P, P, P, P]
         L.cukd_radius_model_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_uint64]
         L.cukd_radius_model_destroy.argtypes = [C.c_void_p]
+        L.cukd_radius_model_set_loss.argtypes = [C.c_void_p, C.c_float]
         L.cukd_radius_model_set_grid.argtypes = [C.c_void_p, P, I64, C.POINTER(Layout), P, P]
         L.cukd_radius_model_train.argtypes = [C.c_void_p, P, P, I64, C.c_int, C.c_int,
                                               C.c_float, P, P]
@@ -413,6 +418,27 @@ def knn_visits(tree, queries, k, method="stack_based", layout=None, world_bounds
     return v
 
 
+def build_check(stream=None):
+    """Waits for the stream and raises CukdError(CUKD_ERR_TIMEOUT) if a
+    build's bounded device-side wait gave up since the last check (that
+    build left its records unchanged) -- cukd_build_check."""
+    _check(lib().cukd_build_check(_stream(stream)), "cukd_build_check")
+
+
+def set_async_wait_polls(polls=None):
+    """Test hook: polls of the builder's first bulk-copy wait (None = the
+    default; 0 gives up at once) -- cukd_set_async_wait_polls."""
+    _check(lib().cukd_set_async_wait_polls(ASYNC_WAIT_POLLS_DEFAULT if polls is None
+                                           else int(polls)), "cukd_set_async_wait_polls")
+
+
+def async_wait_timeouts():
+    """Bulk-copy waits that gave up on this device so far (synchronises)."""
+    c = C.c_uint()
+    _check(lib().cukd_async_wait_timeouts(C.byref(c)), "cukd_async_wait_timeouts")
+    return c.value
+
+
 def launch_count():
     """Kernels launched by the library so far in this process."""
     return int(lib().cukd_launch_count())
@@ -501,10 +527,15 @@ class RadiusModel:
 
     NUM_PARAMS = 4545
 
-    def __init__(self, grid_res=64, seed=0):
+    def __init__(self, grid_res=64, seed=0, quantile=0.0):
+        """quantile: 0 trains with mean squared error (the network predicts
+        the conditional mean of the log k-th distance); 0 < q < 1 with the
+        pinball loss (it predicts that quantile)."""
         self.h = C.c_void_p()
         _check(lib().cukd_radius_model_create(C.byref(self.h), grid_res, seed),
                "cukd_radius_model_create")
+        _check(lib().cukd_radius_model_set_loss(self.h, float(quantile)),
+               "cukd_radius_model_set_loss")
         self.final_loss = None
 
     def __del__(self):

@@ -105,11 +105,18 @@ constexpr int kWideResolveSegs = 16;
 // level_fused_kernel (10M-point build: 5.61 -> 5.43 ms)
 constexpr int64_t kFusedMax = kChunk;
 constexpr uint32_t kWaitPolls = 1u << 22;  // bound of a bulk-copy barrier wait
+static_assert(kWaitPolls == CUKD_ASYNC_WAIT_POLLS_DEFAULT, "documented default");
 // bulk-copy barrier waits that gave up: never expected (the copies read
 // memory the build owns), but a wait that does not complete must end the
-// kernel rather than hang it; the tree of that build is then wrong, and
-// cukd_async_wait_timeouts() reports the count
+// kernel rather than hang it.  The build's status word is then set: every
+// later kernel of that build returns at once and the caller's records are
+// left as they were; cukd_async_wait_timeouts() reports the count and
+// cukd_build_check() turns it into CUKD_ERR_TIMEOUT.
 __device__ unsigned int g_wait_timeouts = 0;
+// polls of the first (staging) wait; cukd_set_async_wait_polls changes it
+// so that a test can make the wait run out (the second wait, which lets the
+// copies in flight land before the CTA exits, always uses kWaitPolls)
+__device__ uint32_t g_wait_polls = kWaitPolls;
 constexpr int kBinPoints = 32;  // target points per histogram bin (global levels)
 
 struct Bufs {
@@ -127,7 +134,19 @@ struct Bufs {
   uint32_t *sel;                  // [seg][3]: pivot bin, count below, pivot-bin count
   uint32_t *cur;                  // [seg][3]: left / right / candidate cursors
   uint32_t *wbmin, *wbmax;        // world bounds as keys, [D]
+  uint32_t *status;               // this build's failure flags (0 = fine)
 };
+
+// A bulk-copy wait of this build gave up: the CTA-uniform answer (the flag
+// can be set by another CTA of the same launch while this one starts).
+// Every thread of the block must call it.
+__device__ __forceinline__ bool build_failed(const Bufs &b)
+{
+  __shared__ uint32_t failed;
+  if (threadIdx.x == 0) failed = b.status ? *(volatile const uint32_t *)b.status : 0u;
+  __syncthreads();
+  return failed != 0;
+}
 
 // ---------------------------------------------------------------------------
 // scalar helpers
@@ -309,6 +328,7 @@ __device__ inline SegGeo seg_geo(const LevelArgs &a, int w)
 template <int SC, int D>
 __global__ void __launch_bounds__(kGThreads) hist_kernel(Bufs b, LevelArgs a)
 {
+  if (build_failed(b)) return;
   __shared__ uint32_t sh[kMaxBins];
   const int groups = (a.chunksPerSeg + kHistGroup - 1) / kHistGroup;
   const int seg = blockIdx.x / groups;
@@ -334,6 +354,7 @@ __global__ void __launch_bounds__(kGThreads) hist_kernel(Bufs b, LevelArgs a)
 // one warp per subtree: the bin that holds rank leftSize(g)
 __global__ void select_kernel(Bufs b, LevelArgs a)
 {
+  if (build_failed(b)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= a.nseg) return;
@@ -369,6 +390,7 @@ __global__ void select_kernel(Bufs b, LevelArgs a)
 // (a warp summing 128 bins per lane was latency bound there)
 __global__ void __launch_bounds__(256) select_block_kernel(Bufs b, LevelArgs a)
 {
+  if (build_failed(b)) return;
   __shared__ uint32_t warpSum[8];
   const int seg = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -442,6 +464,7 @@ constexpr size_t partition_smem()
 template <int SC, int D>
 __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs a)
 {
+  if (build_failed(b)) return;
   constexpr int W = kGThreads / 32;
   constexpr int PER_WARP = kChunk / W;
   constexpr int ROUNDS = PER_WARP / 32;
@@ -481,8 +504,11 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
     for (int d = 0; d < D; d++) bulk_copy_g2s(stage + d * kStageSpan, b.key[cb][d] + a0, bytes, &bar);
     bulk_copy_g2s(stage + D * kStageSpan, b.idx[cb] + a0, bytes, &bar);
   }
-  if (!mbar_wait_bounded(&bar, 0, kWaitPolls)) {
-    if (threadIdx.x == 0) atomicAdd(&g_wait_timeouts, 1u);
+  if (!mbar_wait_bounded(&bar, 0, g_wait_polls)) {
+    if (threadIdx.x == 0) {
+      atomicAdd(&g_wait_timeouts, 1u);
+      atomicOr(b.status, 1u);
+    }
     mbar_wait_bounded(&bar, 0, kWaitPolls);  // let copies in flight land first
     return;
   }
@@ -601,6 +627,7 @@ __global__ void __launch_bounds__(kGThreads) partition_kernel(Bufs b, LevelArgs 
 template <int SC, int D, int NT>
 __global__ void __launch_bounds__(NT) resolve_kernel(Bufs b, LevelArgs a, bool explicitDims)
 {
+  if (build_failed(b)) return;
   __shared__ uint32_t hist[256];
   __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr, sLo, sHi;
   __shared__ uint32_t pw[D + 1];
@@ -819,6 +846,7 @@ template <int SC, int D>
 __global__ void __launch_bounds__(kGThreads) level_fused_kernel(Bufs b, LevelArgs a,
                                                                 bool explicitDims)
 {
+  if (build_failed(b)) return;
   extern __shared__ __align__(128) uint32_t stage[];  // [D + 1][kStageSpan]
   __shared__ uint32_t hist[256];
   __shared__ uint32_t sDigit, sCount, sRank, sPivot, sNl, sNr;
@@ -860,8 +888,11 @@ __global__ void __launch_bounds__(kGThreads) level_fused_kernel(Bufs b, LevelArg
     for (int d = 0; d < D; d++) bulk_copy_g2s(stage + d * kStageSpan, b.key[cb][d] + a0, bytes, &bar);
     bulk_copy_g2s(stage + D * kStageSpan, b.idx[cb] + a0, bytes, &bar);
   }
-  if (!mbar_wait_bounded(&bar, 0, kWaitPolls)) {
-    if (tid == 0) atomicAdd(&g_wait_timeouts, 1u);
+  if (!mbar_wait_bounded(&bar, 0, g_wait_polls)) {
+    if (tid == 0) {
+      atomicAdd(&g_wait_timeouts, 1u);
+      atomicOr(b.status, 1u);
+    }
     mbar_wait_bounded(&bar, 0, kWaitPolls);  // let copies in flight land first
     return;
   }
@@ -1541,6 +1572,7 @@ template <int SC, int D>
 __global__ void __launch_bounds__(kSubThreads, 4) subtree_kernel(Bufs b, int64_t n, int L0, int cb,
                                                               bool explicitDims)
 {
+  if (build_failed(b)) return;
   extern __shared__ __align__(16) uint8_t smem_raw[];
   SubSmem<D, kTile, kSubThreads> &S =
       *reinterpret_cast<SubSmem<D, kTile, kSubThreads> *>(smem_raw);
@@ -1566,6 +1598,7 @@ template <int D, int TILE>
 __global__ void __launch_bounds__(ForestNT<TILE>::value, ForestNT<TILE>::minBlocks)
     subtree_forest_kernel(Bufs b, ForestSubtrees f)
 {
+  if (build_failed(b)) return;
   constexpr int NT = ForestNT<TILE>::value;
   extern __shared__ __align__(16) uint8_t smem_raw[];
   SubSmem<D, TILE, NT> &S = *reinterpret_cast<SubSmem<D, TILE, NT> *>(smem_raw);
@@ -1592,8 +1625,10 @@ __global__ void __launch_bounds__(256) finalize_kernel(uint8_t *__restrict__ pts
                                                        const uint32_t *__restrict__ perm,
                                                        const uint8_t *__restrict__ ndim,
                                                        int64_t n, int stride, int doff,
-                                                       int dshift, uint32_t dmask)
+                                                       int dshift, uint32_t dmask,
+                                                       const uint32_t *status)
 {
+  if (*status) return;  // a wait gave up: leave the caller's records as they were
   const int words = stride >> 2;
   for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < n;
        g += int64_t(gridDim.x) * blockDim.x) {
@@ -1619,12 +1654,14 @@ static int pow2ceil(int64_t v)
   return p;
 }
 
-template <int SC, int D>
-int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st,
-               const cukd_mem_resource *mem)
+// The builder's launch sequence; Arena provides alloc(T **, count) -- the
+// caller's memory resource (TempArena) or the allocation-free builder's fixed
+// device scratch (StaticCarver) -- so both entry points run the same code.
+template <int SC, int D, class Arena>
+int build_run(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st,
+              Arena &arena)
 {
   const bool explicitDims = L.doff >= 0;
-  TempArena arena(st, mem);
   Bufs b = {};
   int G = 0;
   while (subtree_size((int64_t(1) << G) - 1, n) > kTile) G++;
@@ -1658,7 +1695,10 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
   CKB_TRY(arena.alloc(&b.cur, capSeg * 3));
   CKB_TRY(arena.alloc(&b.wbmin, D));
   CKB_TRY(arena.alloc(&b.wbmax, D));
+  CKB_TRY(arena.alloc(&b.status, 1));
 
+  // what must start filled / zeroed is reset here, on the caller's stream
+  CKB_CUDA(cudaMemsetAsync(b.status, 0, sizeof(uint32_t), st));
   CKB_CUDA(cudaMemsetAsync(b.perm, 0xff, sizeof(uint32_t) * n, st));
   CKB_CUDA(cudaMemsetAsync(b.wbmin, 0xff, sizeof(uint32_t) * D, st));
   CKB_CUDA(cudaMemsetAsync(b.wbmax, 0, sizeof(uint32_t) * D, st));
@@ -1724,10 +1764,19 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
   {
     const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 16));
     finalize_kernel<<<blocks, 256, 0, st>>>((uint8_t *)pts, orig, b.perm, b.ndim, n, L.stride,
-                                            explicitDims ? L.doff : -1, L.dshift, L.dmask);
+                                            explicitDims ? L.doff : -1, L.dshift, L.dmask,
+                                            b.status);
     CKB_CHECK_LAUNCH();
   }
   return CUKD_OK;
+}
+
+template <int SC, int D>
+int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st,
+               const cukd_mem_resource *mem)
+{
+  TempArena arena(st, mem);
+  return build_run<SC, D>(pts, n, L, worldBounds, st, arena);
 }
 
 template <int SC, int D>
@@ -1827,139 +1876,62 @@ struct StaticCarver {
   }
 };
 
-// Device address of the scratch on the current device, looked up once per
-// device (host code may not use the symbol's name as a device address).
+// The driver's handle of the current context (cuCtxGetCurrent, reached
+// through the runtime so the library links no driver library).
+static void *current_context()
+{
+  using Fn = int (*)(void **);
+  static Fn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return (Fn)p;
+  }();
+  void *ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of the scratch in the current context, looked up once per
+// (device, context): host code may not use the symbol's name as a device
+// address, and an address belongs to the context it was looked up in (a
+// device reset or another context on the device needs a new lookup).
 static int noalloc_scratch_ptr(uint8_t **out)
 {
   static std::mutex mu;
   static void *ptrs[64] = {};
+  static void *ctxs[64] = {};
   int dev = 0;
   CKB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return CUKD_ERR_UNSUPPORTED;
+  void *ctx = current_context();
   std::lock_guard<std::mutex> lock(mu);
-  if (!ptrs[dev]) {
+  if (!ptrs[dev] || !ctx || ctx != ctxs[dev]) {
     void *p = nullptr;
+    // (makes the device's primary context current when none is)
     CKB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     if (!p) return CUKD_ERR_CUDA;
     ptrs[dev] = p;
+    ctxs[dev] = current_context();
   }
   *out = (uint8_t *)ptrs[dev];
   return CUKD_OK;
 }
 
-// The launch sequence of build_impl with every buffer carved from the
-// static scratch (and no memory-pool calls).
+// The builder's launch sequence with every buffer carved from the static
+// scratch (and no memory-pool calls).
 template <int SC, int D>
 int build_impl_static(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStream_t st)
 {
-  const bool explicitDims = L.doff >= 0;
   StaticCarver arena;
   CKB_TRY(noalloc_scratch_ptr(&arena.base));
   arena.cap = kNoAllocScratchBytes;
   arena.used = 0;
-  Bufs b = {};
-  int G = 0;
-  while (subtree_size((int64_t(1) << G) - 1, n) > kTile) G++;
-  const int64_t capSeg = int64_t(1) << G;
-  for (int x = 0; x < 2; x++) {
-    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.key[x][d], n));
-    CKB_TRY(arena.alloc(&b.idx[x], n));
-  }
-  if (G > 0) {
-    for (int d = 0; d < D; d++) CKB_TRY(arena.alloc(&b.ckey[d], n));
-    CKB_TRY(arena.alloc(&b.cidx, n));
-  }
-  CKB_TRY(arena.alloc(&b.perm, n));
-  CKB_TRY(arena.alloc(&b.ndim, n));
-  uint8_t *orig = nullptr;
-  CKB_TRY(arena.alloc(&orig, size_t(n) * L.stride));
-  for (int x = 0; x < 2; x++) {
-    CKB_TRY(arena.alloc(&b.sdim[x], capSeg));
-    CKB_TRY(arena.alloc(&b.sbmin[x], capSeg * D));
-    CKB_TRY(arena.alloc(&b.sbmax[x], capSeg * D));
-    CKB_TRY(arena.alloc(&b.sbox[x], capSeg * 2 * D));
-  }
-  int64_t histCap = 64;
-  for (int lvl = 0; lvl < G; lvl++) {
-    const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
-    const int nb = level_bins(maxSeg);
-    histCap = std::max(histCap, (int64_t(1) << lvl) * nb);
-  }
-  CKB_TRY(arena.alloc(&b.hist, histCap));
-  CKB_TRY(arena.alloc(&b.sel, capSeg * 3));
-  CKB_TRY(arena.alloc(&b.cur, capSeg * 3));
-  CKB_TRY(arena.alloc(&b.wbmin, D));
-  CKB_TRY(arena.alloc(&b.wbmax, D));
-
-  // what must start filled / zeroed is reset here, on the caller's stream
-  CKB_CUDA(cudaMemsetAsync(b.perm, 0xff, sizeof(uint32_t) * n, st));
-  CKB_CUDA(cudaMemsetAsync(b.wbmin, 0xff, sizeof(uint32_t) * D, st));
-  CKB_CUDA(cudaMemsetAsync(b.wbmax, 0, sizeof(uint32_t) * D, st));
-  {
-    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 8));
-    extract_kernel<SC, D><<<blocks, 256, 0, st>>>((const uint8_t *)pts, n, L.stride, L.poff,
-                                                  orig, b);
-    CKB_CHECK_LAUNCH();
-  }
-  root_kernel<SC, D><<<1, 32, 0, st>>>(b, worldBounds, explicitDims);
-  CKB_CHECK_LAUNCH();
-  if (G > 0) CKB_TRY((partition_opt_in<SC, D>()));
-  int cb = 0;
-  for (int lvl = 0; lvl < G; lvl++) {
-    const int nseg = 1 << lvl;
-    const int64_t maxSeg = subtree_size((int64_t(1) << lvl) - 1, n);
-    LevelArgs a{};
-    a.n = n;
-    a.level = lvl;
-    a.nb = level_bins(maxSeg);
-    a.chunksPerSeg = int(div_up(maxSeg, kChunk));
-    a.nseg = nseg;
-    a.cb = cb;
-    CKB_CUDA(cudaMemsetAsync(b.sbmin[1], 0xff, sizeof(uint32_t) * 2 * nseg * D, st));
-    CKB_CUDA(cudaMemsetAsync(b.sbmax[1], 0, sizeof(uint32_t) * 2 * nseg * D, st));
-    if (maxSeg <= kFusedMax) {
-      level_fused_kernel<SC, D><<<nseg, kGThreads, partition_smem<D>(), st>>>(b, a, explicitDims);
-      CKB_CHECK_LAUNCH();
-    } else {
-      CKB_CUDA(cudaMemsetAsync(b.hist, 0, sizeof(uint32_t) * size_t(nseg) * a.nb, st));
-      const int64_t grid = int64_t(nseg) * a.chunksPerSeg;
-      hist_kernel<SC, D><<<unsigned(int64_t(nseg) * div_up(a.chunksPerSeg, kHistGroup)), kGThreads, 0,
-                           st>>>(b, a);
-      CKB_CHECK_LAUNCH();
-      if (a.nb >= 512)
-        select_block_kernel<<<unsigned(nseg), 256, 0, st>>>(b, a);
-      else
-        select_kernel<<<unsigned(div_up(int64_t(nseg) * 32, 256)), 256, 0, st>>>(b, a);
-      CKB_CHECK_LAUNCH();
-      partition_kernel<SC, D><<<unsigned(grid), kGThreads, partition_smem<D>(), st>>>(b, a);
-      CKB_CHECK_LAUNCH();
-      if (nseg <= kWideResolveSegs)
-        resolve_kernel<SC, D, 1024><<<nseg, 1024, 0, st>>>(b, a, explicitDims);
-      else
-        resolve_kernel<SC, D, kGThreads><<<nseg, kGThreads, 0, st>>>(b, a, explicitDims);
-      CKB_CHECK_LAUNCH();
-    }
-    cb ^= 1;
-    std::swap(b.sdim[0], b.sdim[1]);
-    std::swap(b.sbmin[0], b.sbmin[1]);
-    std::swap(b.sbmax[0], b.sbmax[1]);
-    std::swap(b.sbox[0], b.sbox[1]);
-  }
-  {
-    const size_t smem = sizeof(SubSmem<D, kTile, kSubThreads>);
-    CKB_CUDA(cudaFuncSetAttribute(subtree_kernel<SC, D>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    subtree_kernel<SC, D><<<unsigned(capSeg), kSubThreads, smem, st>>>(b, n, G, cb,
-                                                                       explicitDims);
-    CKB_CHECK_LAUNCH();
-  }
-  {
-    const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 16));
-    finalize_kernel<<<blocks, 256, 0, st>>>((uint8_t *)pts, orig, b.perm, b.ndim, n, L.stride,
-                                            explicitDims ? L.doff : -1, L.dshift, L.dmask);
-    CKB_CHECK_LAUNCH();
-  }
-  return CUKD_OK;
+  return build_run<SC, D>(pts, n, L, worldBounds, st, arena);
 }
 
 // ---------------------------------------------------------------------------
@@ -2044,6 +2016,7 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
   const int64_t n = f.total;
   const int stride = 4 * D;
   if (n == 0) return CUKD_OK;
+  CKB_CUDA(cudaMemsetAsync(b.status, 0, sizeof(uint32_t), st));
   CKB_CUDA(cudaMemsetAsync(b.wbmin, 0xff, sizeof(uint32_t) * D, st));
   CKB_CUDA(cudaMemsetAsync(b.wbmax, 0, sizeof(uint32_t) * D, st));
   {
@@ -2134,7 +2107,7 @@ int forest_build_impl(const ForestBuild &f, float *pts, float *boundsOut, cudaSt
   {
     const int blocks = int(std::min<int64_t>(div_up(n, 256), kNumSMs * 16));
     finalize_kernel<<<blocks, 256, 0, st>>>((uint8_t *)pts, ws->orig, b.perm, b.ndim, n, stride,
-                                            -1, 0, 0u);
+                                            -1, 0, 0u, b.status);
     CKB_CHECK_LAUNCH();
   }
   return CUKD_OK;
@@ -2217,6 +2190,7 @@ int forest_workspace_create(ForestBuild *f, int64_t maxItems, int64_t histCap)
   T(get(&b.cur, items * 3));
   T(get(&b.wbmin, D));
   T(get(&b.wbmax, D));
+  T(get(&b.status, 1));
   f->ws = ws;
   if (rc != CUKD_OK) forest_workspace_destroy(f);
   return rc;
@@ -2377,6 +2351,28 @@ int cukd_async_wait_timeouts(unsigned int *count)
   if (!count) return CUKD_ERR_INVALID_ARGUMENT;
   CKB_CUDA(cudaMemcpyFromSymbol(count, ckb::build::g_wait_timeouts, sizeof(unsigned int)));
   return CUKD_OK;
+}
+
+int cukd_set_async_wait_polls(uint32_t polls)
+{
+  CKB_CUDA(cudaMemcpyToSymbol(ckb::build::g_wait_polls, &polls, sizeof(uint32_t)));
+  return CUKD_OK;
+}
+
+int cukd_build_check(cudaStream_t stream)
+{
+  static std::mutex mu;
+  static unsigned int seen[64] = {};
+  int dev = 0;
+  CKB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return CUKD_ERR_UNSUPPORTED;
+  CKB_CUDA(cudaStreamSynchronize(stream));
+  unsigned int count = 0;
+  CKB_CUDA(cudaMemcpyFromSymbol(&count, ckb::build::g_wait_timeouts, sizeof(unsigned int)));
+  std::lock_guard<std::mutex> lock(mu);
+  const bool gaveUp = count != seen[dev];
+  seen[dev] = count;
+  return gaveUp ? CUKD_ERR_TIMEOUT : CUKD_OK;
 }
 
 }  // extern "C"

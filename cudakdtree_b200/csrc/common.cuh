@@ -72,21 +72,23 @@ struct TempArena {
     size_t bytes = count * sizeof(T);
     if (bytes == 0) bytes = 16;
     bytes = (bytes + 255) & ~size_t(255);
+    void *use = nullptr;
     if (mem && mem->alloc) {
-      if (mem->alloc(mem->ctx, &p, bytes, stream) != 0 || !p) return CUKD_ERR_OUT_OF_MEMORY;
-      if (reinterpret_cast<uintptr_t>(p) & 15u) {  // bulk copies need 16-byte alignment
-        if (mem->release) mem->release(mem->ctx, p, stream);
-        return CUKD_ERR_INVALID_ARGUMENT;
-      }
+      // the builder's bulk copies need 16-byte-aligned arrays, and a caller's
+      // pool may hand out less: ask for 16 bytes more and align up (the
+      // block's own pointer is what goes back to the pool)
+      if (mem->alloc(mem->ctx, &p, bytes + 16, stream) != 0 || !p) return CUKD_ERR_OUT_OF_MEMORY;
+      use = reinterpret_cast<void *>((reinterpret_cast<uintptr_t>(p) + 15u) & ~uintptr_t(15));
     } else {
       cudaError_t e = cudaMallocAsync(&p, bytes, stream);
       if (e != cudaSuccess) {
         cudaGetLastError();
         return e == cudaErrorMemoryAllocation ? CUKD_ERR_OUT_OF_MEMORY : CUKD_ERR_CUDA;
       }
+      use = p;
     }
     ptrs.push_back(p);
-    *out = (T *)p;
+    *out = (T *)use;
     return CUKD_OK;
   }
   void release_all()

@@ -133,10 +133,12 @@ struct TrainSmem {
   float y[S], dy[S];
 };
 
+// quantile == 0: mean squared error; 0 < quantile < 1: pinball loss, whose
+// minimiser is that quantile of the target given the features
 __global__ void __launch_bounds__(kTrainThreads) train_kernel(
     const __nv_bfloat16 *__restrict__ wbf, const float *__restrict__ feat,
     const float *__restrict__ tgt, int64_t begin, int64_t count, float gradScale, float *grad,
-    float *lossOut)
+    float *lossOut, float quantile)
 {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   TrainSmem &M = *reinterpret_cast<TrainSmem *>(smem_raw);
@@ -188,8 +190,16 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
         const float y = p + M.b3;
         const float e = s < ns ? y - tgt[s0 + s] : 0.f;
         M.y[s] = y;
-        M.dy[s] = 2.f * e * gradScale;
-        if (s < ns && lossOut) atomicAdd(lossOut, e * e);
+        float dl, l;
+        if (quantile > 0.f) {  // pinball: slope 1 - q above the target, -q below
+          dl = e > 0.f ? 1.f - quantile : (e < 0.f ? -quantile : 0.f);
+          l = e > 0.f ? (1.f - quantile) * e : -quantile * e;
+        } else {
+          dl = 2.f * e;
+          l = e * e;
+        }
+        M.dy[s] = dl * gradScale;
+        if (s < ns && lossOut) atomicAdd(lossOut, l);
       }
     }
   }
@@ -348,6 +358,7 @@ struct cukd_radius_model_s {
   ckb::learned::ModelDev d;
   int trained;
   float last_loss;
+  float quantile;  // training loss: 0 = mean squared error, else pinball at this quantile
 };
 
 using namespace ckb;
@@ -390,6 +401,15 @@ int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t see
   CKB_CUDA(cudaMemset(m->d.v, 0, sizeof(float) * NP));
   CKB_CUDA(cudaMemset(m->d.grad, 0, sizeof(float) * NP));
   *out = (cukd_radius_model *)m;
+  return CUKD_OK;
+}
+
+int cukd_radius_model_set_loss(cukd_radius_model *model, float quantile)
+{
+  auto *m = (cukd_radius_model_s *)model;
+  if (!m || !(quantile == 0.f || (quantile > 0.f && quantile < 1.f)))
+    return CUKD_ERR_INVALID_ARGUMENT;
+  m->quantile = quantile;
   return CUKD_OK;
 }
 
@@ -487,7 +507,8 @@ int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
     for (int64_t b0 = 0; b0 < nq; b0 += batch) {
       const int64_t cnt = std::min<int64_t>(batch, nq - b0);
       train_kernel<<<unsigned(div_up(cnt, S)), kTrainThreads, smem, st>>>(
-          m->d.wbf, feat, tgt, b0, cnt, 1.f / float(cnt), m->d.grad, last ? m->d.loss : nullptr);
+          m->d.wbf, feat, tgt, b0, cnt, 1.f / float(cnt), m->d.grad, last ? m->d.loss : nullptr,
+          m->quantile);
       CKB_CHECK_LAUNCH();
       step++;
       const float c1 = 1.f - std::pow(b1, float(step)), c2 = 1.f - std::pow(b2, float(step));
@@ -532,7 +553,7 @@ int cukd_radius_model_gradients(cukd_radius_model *model, const float *d_feature
   CKB_CUDA(cudaMemsetAsync(m->d.grad, 0, sizeof(float) * NP, st));
   CKB_CUDA(cudaMemsetAsync(m->d.loss, 0, sizeof(float) * 2, st));
   train_kernel<<<unsigned(div_up(n, S)), kTrainThreads, smem, st>>>(
-      m->d.wbf, d_features, d_targets, 0, n, 1.f / float(n), m->d.grad, m->d.loss);
+      m->d.wbf, d_features, d_targets, 0, n, 1.f / float(n), m->d.grad, m->d.loss, m->quantile);
   CKB_CHECK_LAUNCH();
   if (h_grad)
     CKB_CUDA(cudaMemcpyAsync(h_grad, m->d.grad, sizeof(float) * NP, cudaMemcpyDeviceToHost, st));

@@ -88,6 +88,9 @@ void build(data_t *d_points, int numPoints, box_t<typename traits::point_t> *wor
   if (plain) {
     const cukd_layout l = layout_of<point_t>(int(sizeof(data_t)), -1);
     check(cukd_build_tree(d_points, numPoints, &l, worldBounds, builder, stream, &c), name);
+    // like the reference's builders, return after the work is done and
+    // throw if it failed (a bounded device-side wait that gave up)
+    check(cukd_build_check(stream), name);
     return;
   }
   ShimRecord<point_t> *rec = nullptr;
@@ -109,6 +112,7 @@ void build(data_t *d_points, int numPoints, box_t<typename traits::point_t> *wor
   mr.free(rec, stream);
   mr.free(copy, stream);
   check(rc, name);
+  check(cukd_build_check(stream), name);
 }
 
 }  // namespace detail

@@ -85,9 +85,9 @@ typedef struct cukd_layout {
  * upper[num_dims], of the scalar type. */
 
 /* Memory resource: reference GpuMemoryResource (cukd/helpers.h:30-33).
- * Blocks must be at least 16-byte aligned (cudaMalloc-style allocators give
- * 256; the builder stages its arrays with 16-byte bulk copies): a misaligned
- * block makes the call return CUKD_ERR_INVALID_ARGUMENT. */
+ * Any alignment works: each request asks for 16 bytes more than it uses and
+ * aligns the block up itself (the builder stages its arrays with 16-byte
+ * bulk copies); release receives the pointer alloc returned. */
 typedef struct cukd_mem_resource {
   void *ctx;
   int (*alloc)(void *ctx, void **ptr, size_t bytes, cudaStream_t stream); /* 0 = ok */
@@ -368,10 +368,18 @@ CUKD_API int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_
                                         int64_t n, const cukd_layout *layout,
                                         const float *h_world_bounds, cudaStream_t stream);
 
+/* Training loss of later cukd_radius_model_train / _gradients calls on the
+ * standardised log distance: quantile 0 (the default) = mean squared error,
+ * so the network predicts the conditional mean; 0 < quantile < 1 = pinball
+ * loss, so it predicts that quantile of the k-th distance given the
+ * features -- a larger safety margin where the features say less, fewer
+ * fallbacks to the plain traversal at the same radius scale. */
+CUKD_API int cukd_radius_model_set_loss(cukd_radius_model *model, float quantile);
+
 /* Trains on nq queries and their exact k-th squared distances (for example
  * the knn() return values of cukd_knn): Adam on minibatches, `epochs`
  * passes; *h_final_loss receives the last epoch's mean squared error on the
- * standardised log distance. */
+ * standardised log distance (or the pinball loss, cukd_radius_model_set_loss). */
 CUKD_API int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
                                      const float *d_kth_d2, int64_t nq, int epochs, int batch,
                                      float lr, float *h_final_loss, cudaStream_t stream);
@@ -485,9 +493,24 @@ CUKD_API unsigned long long cukd_launch_count(void);
 /* number of bounded waits on bulk-copy barriers (the builder's partition
  * pass) that gave up on the current device since the library was loaded;
  * 0 unless something is badly wrong -- a kernel ends instead of hanging,
- * and the tree of that build is then invalid.  Synchronises the device.
- * No reference counterpart. */
+ * and that build stops, leaving the caller's records unchanged.
+ * Synchronises the device.  No reference counterpart. */
 CUKD_API int cukd_async_wait_timeouts(unsigned int *count);
+
+/* Synchronises `stream` and returns CUKD_ERR_TIMEOUT if a bulk-copy wait of
+ * a build on the current device gave up since the previous check (that
+ * build stopped and left the caller's records exactly as they were), else
+ * CUKD_OK.  The reference's builders synchronise and throw on failure
+ * (builder_thrust.h:479-511, common.h:276-285); the C++ shim's buildTree
+ * calls this after the build to do the same. */
+CUKD_API int cukd_build_check(cudaStream_t stream);
+
+/* Test hook: how many times the builder's first bulk-copy wait polls its
+ * barrier before giving up, on the current device (default
+ * CUKD_ASYNC_WAIT_POLLS_DEFAULT; 0 gives up at once, so that a test can make
+ * the wait run out without any fault).  Synchronous. */
+#define CUKD_ASYNC_WAIT_POLLS_DEFAULT 4194304u
+CUKD_API int cukd_set_async_wait_polls(uint32_t polls);
 
 #ifdef __cplusplus
 }

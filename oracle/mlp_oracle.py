@@ -51,17 +51,22 @@ def forward(p, f, bf16_act=True):
     return y, (h1, h2)
 
 
-def loss_and_grad(p, f, t, bf16_act=True):
-    """Mean squared error and its gradient w.r.t. the parameter vector (the
-    bf16 roundings pass gradients straight through, as on the GPU)."""
+def loss_and_grad(p, f, t, bf16_act=True, quantile=0.0):
+    """Mean squared error (quantile 0) or mean pinball loss at `quantile`, and
+    its gradient w.r.t. the parameter vector (the bf16 roundings pass
+    gradients straight through, as on the GPU)."""
     f = bf16(f) if bf16_act else np.asarray(f, np.float64)
     t = np.asarray(t, np.float64)
     W1, b1, W2, b2, w3, b3 = unpack(p)
     y, (h1, h2) = forward(p, f, bf16_act)
     n = len(t)
     e = y - t
-    loss = float(np.mean(e * e))
-    dy = 2 * e / n
+    if quantile > 0:
+        loss = float(np.mean(np.where(e > 0, (1 - quantile) * e, -quantile * e)))
+        dy = np.where(e > 0, 1 - quantile, np.where(e < 0, -quantile, 0.0)) / n
+    else:
+        loss = float(np.mean(e * e))
+        dy = 2 * e / n
     g = np.zeros(NP)
     g[OW3:OB3] = h2.T @ dy
     g[OB3] = dy.sum()

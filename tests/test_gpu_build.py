@@ -199,35 +199,67 @@ def test_partition_staging_waits_never_give_up():
     assert count.value == 0
 
 
-def test_misaligned_memory_resource_is_rejected_before_any_launch():
-    """A caller memory resource must hand out 16-byte-aligned blocks (the
-    partition pass stages them with bulk copies); a block 4 bytes off is
-    refused with CUKD_ERR_INVALID_ARGUMENT before any kernel runs, and the
-    points are left untouched."""
+@pytest.mark.parametrize("offset", [4, 8, 12])
+def test_memory_resource_with_any_alignment_builds_the_same_tree(offset):
+    """A caller memory resource whose blocks are only 4-byte aligned (the
+    reference's GpuMemoryResource makes no alignment promise,
+    helpers.h:31-34): the builder aligns each block up itself, builds the
+    oracle's tree, and hands every block back with the pointer it got."""
     import ctypes as C
     live = {}
+    released = []
 
     def alloc(ctx, out, nbytes, stream):
         t = torch.empty(int(nbytes) + 64, dtype=torch.uint8, device="cuda")
-        p = t.data_ptr() + 4
+        p = t.data_ptr() + offset
         live[p] = t
         out[0] = p
         return 0
 
     def release(ctx, ptr, stream):
+        released.append(ptr)
         live.pop(ptr, None)
         return 0
 
     a_fn = ck._ALLOC_FN(alloc)
     r_fn = ck._RELEASE_FN(release)
     mr = ck.MemResource(None, C.cast(a_fn, C.c_void_p), C.cast(r_fn, C.c_void_p))
-    n = 5000
-    pts = make_points(n, 3, "uniform", seed=11)
+    n = 50000
+    pts = make_points(n, 3, "tie", seed=11)
     t = torch.from_numpy(pts).cuda()
-    before = t.clone()
     lay = ck.layout_for("float32", 3)
     rc = ck.lib().cukd_build_tree(t.data_ptr(), n, C.byref(lay), None, 0, None, C.byref(mr))
     torch.cuda.synchronize()
-    assert rc == 1  # CUKD_ERR_INVALID_ARGUMENT
-    assert torch.equal(t, before)
-    assert not live  # the misaligned block was handed back
+    assert rc == 0
+    perm, _, _ = po.build(pts)
+    assert np.array_equal(t.cpu().numpy(), pts[perm])
+    assert released and not live  # every block came back, by its own pointer
+
+
+def test_wait_that_runs_out_leaves_the_points_and_reports_timeout():
+    """The partition pass's bounded bulk-copy wait, made to give up at once
+    (poll bound 0 through the test hook; the copies still land before the
+    CTAs leave): the build stops, every later kernel of it returns at once,
+    the caller's records are left exactly as they were, and cukd_build_check
+    reports CUKD_ERR_TIMEOUT.  With the default bound restored the next
+    build is the oracle's tree again."""
+    n = 300000
+    pts = make_points(n, 3, "gmm", seed=5)
+    ck.build_check()  # clean slate
+    before = ck.async_wait_timeouts()
+    ck.set_async_wait_polls(0)
+    try:
+        t = torch.from_numpy(pts).cuda()
+        ck.build_tree(t)
+        with pytest.raises(ck.CukdError) as err:
+            ck.build_check()
+        assert err.value.status == 6  # CUKD_ERR_TIMEOUT
+        assert np.array_equal(t.cpu().numpy(), pts)
+        assert ck.async_wait_timeouts() > before
+    finally:
+        ck.set_async_wait_polls()
+    t = torch.from_numpy(pts).cuda()
+    ck.build_tree(t)
+    ck.build_check()
+    perm, _, _ = po.build(pts)
+    assert np.array_equal(t.cpu().numpy(), pts[perm])

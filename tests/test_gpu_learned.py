@@ -23,15 +23,17 @@ def _tree(n, seed=3):
     return pts, rec, wb
 
 
-def test_gradients_match_cpu_oracle():
+@pytest.mark.parametrize("quantile", [0.0, 0.8])
+def test_gradients_match_cpu_oracle(quantile):
     _, rec, wb = _tree(20000)
-    m = ck.RadiusModel(seed=7)
+    m = ck.RadiusModel(seed=7, quantile=quantile)
     m.set_grid(rec, LAYOUT, wb)
     q = torch.from_numpy(wl.mixed_queries(3000, seed=11)).cuda()
     f = m.features(q)
     t = torch.randn(3000, generator=torch.Generator().manual_seed(0)).cuda()
     g, p, loss = m.gradients(f, t)
-    ref_loss, ref_g = mlp_oracle.loss_and_grad(p, f.cpu().numpy(), t.cpu().numpy())
+    ref_loss, ref_g = mlp_oracle.loss_and_grad(p, f.cpu().numpy(), t.cpu().numpy(),
+                                               quantile=quantile)
     assert abs(loss - ref_loss) <= 1e-4 * max(1.0, abs(ref_loss))
     # FP32 accumulation vs float64: relative to the gradient's scale
     scale = np.abs(ref_g).max()

@@ -228,6 +228,26 @@ def test_mlp_oracle_gradient_matches_finite_differences():
         assert abs((lp - lm) / 2e-6 - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
 
 
+@pytest.mark.parametrize("quantile", [0.3, 0.8])
+def test_mlp_oracle_pinball_gradient_matches_finite_differences(quantile):
+    """The pinball-loss gradient (quantile training) against central finite
+    differences, away from the kinks (no target within the step of a
+    prediction)."""
+    from oracle import mlp_oracle as mo
+    rng = np.random.default_rng(1)
+    p = rng.normal(0, 0.3, mo.NP)
+    f = rng.normal(0, 1, (16, 4))
+    y, _ = mo.forward(p, f, bf16_act=False)
+    t = y + rng.choice([-1.0, 1.0], 16) * rng.uniform(0.1, 1.0, 16)
+    _, g = mo.loss_and_grad(p, f, t, bf16_act=False, quantile=quantile)
+    for i in [0, 5, mo.OB1 + 3, mo.OW2 + 100, mo.OW2 + 4000, mo.OB2 + 7, mo.OW3 + 9, mo.OB3]:
+        e = np.zeros(mo.NP)
+        e[i] = 1e-6
+        lp, _ = mo.loss_and_grad(p + e, f, t, bf16_act=False, quantile=quantile)
+        lm, _ = mo.loss_and_grad(p - e, f, t, bf16_act=False, quantile=quantile)
+        assert abs((lp - lm) / 2e-6 - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
+
+
 def test_mlp_oracle_bf16_rounding():
     """The oracle's bf16 rounding (of the tensor-core operands) against
     torch's bfloat16 conversion, ties included."""

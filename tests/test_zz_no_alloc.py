@@ -63,6 +63,29 @@ def test_noalloc_matches_allocating_builder_on_consecutive_calls():
         assert torch.equal(wb, wb_ref)
 
 
+@pytest.mark.parametrize("scalar", ["float32", "int32"])
+def test_noalloc_at_its_documented_limit(scalar):
+    """The largest input the fixed scratch is documented to take: 262144
+    records of 64 bytes with D = 4 and explicit dims, float and int, twice
+    in a row, each equal to the allocating builder's tree."""
+    n, D, stride = 262144, 4, 64
+    words = stride // 4
+    for seed in (1, 2):
+        pts = make_points(n, D, "uniform", scalar=scalar, seed=seed)
+        rec = np.zeros((n, words), np.int32)
+        rec[:, :D] = pts.view(np.int32)
+        rec[:, D + 1] = np.arange(n, dtype=np.int32)
+        lay = ck.layout_for(scalar, D, stride=stride, dim_offset=4 * D, dim_bits=32)
+        ref = torch.from_numpy(rec).cuda()
+        wb_ref = ck.build_tree(ref, layout=lay)
+        got = torch.from_numpy(rec).cuda()
+        wb = torch.empty((2, D), dtype=wb_ref.dtype, device="cuda")
+        assert _noalloc(got, lay, n, wb) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(got, ref), f"tree differs ({scalar}, call {seed})"
+        assert torch.equal(wb, wb_ref)
+
+
 def test_noalloc_rejects_inputs_beyond_its_scratch():
     n = 262145
     t = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
