@@ -896,6 +896,36 @@ def config_c4(ck, dev, peak):
 F4_STRIDE = 32
 
 
+def _learned_side_by_side(ck, P, Q, k, plain_ms, ids, d2, lay, wb, n, qtrain, num_dims, grid_res):
+    """The learned radius on a configuration's tree beside its plain kNN:
+    trained on 1M queries of the serving distribution, radius x1.2; the
+    answers must equal the plain ones (held in ids / d2)."""
+    import torch
+    timed = _timer()
+    ref_ids, ref_d2 = ids.clone(), d2.clone()
+    model = ck.RadiusModel(grid_res=grid_res, seed=1, quantile=LEARNED_QUANTILE,
+                           num_dims=num_dims)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    model.fit(P, qtrain, k, layout=lay, world_bounds=wb, epochs=10, batch=4096)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    fb = [None]
+
+    def run():
+        fb[0] = ck.knn_learned(P, Q, k, model, "stack_based", layout=lay, world_bounds=wb, n=n,
+                               scale=1.2, out_ids=ids, out_d2=d2)[2]
+    t = timed(run, reps=1)
+    same = bool(torch.equal(ids, ref_ids) and torch.equal(d2, ref_d2))
+    nq = Q.shape[0]
+    return {"plain_knn_ms": round(plain_ms, 3), "learned_knn_ms": round(t, 3),
+            "learned_queries_per_s": round(nq / (t / 1e3), 1),
+            "learned_speedup_vs_plain": round(plain_ms / t, 3),
+            "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
+            "identical_results": same, "train_s": round(train_s, 3),
+            "model": f"{num_dims}-D grid {grid_res}^{num_dims}, pinball q={LEARNED_QUANTILE}"}
+
+
 def config_c5(ck, dev, peak):
     """100M float4 points (xyz U[0,1), w N(0,1)) with widest-extent dims in
     the reference's 32-byte {float4; int dim} record, and 20M int3 points in
@@ -931,7 +961,9 @@ def config_c5(ck, dev, peak):
     kb, mv = _knn_bytes(ck, P, Q[:1_000_000], k, F4_STRIDE, 16, scale=nq // 1_000_000,
                         layout=lay, world_bounds=wb, n=n)
     out["float4_knn64_frac"] = _frac(kb, t, peak)
-    out["float4_learned"] = "unavailable: the learned radius model is float3-only"
+    out["float4_learned"] = _learned_side_by_side(
+        ck, P, Q, k, t, ids, d2, lay, wb, n,
+        torch.from_numpy(wl.wide_float4(1_000_000, seed=11)).to(dev), num_dims=4, grid_res=32)
     del P, Q, ids, d2
     torch.cuda.empty_cache()
     pi = wl.int3_points(20_000_000, seed=8)
@@ -945,12 +977,18 @@ def config_c5(ck, dev, peak):
     out["int3_20M_build_ms"] = round(bms, 3)
     out["int3_build_frac"] = _frac(2 * len(pi) * 12 * (int(np.log2(len(pi))) + 1), bms, peak)
     Qi = torch.from_numpy(qi).to(dev)
-    t = timed(lambda: ck.knn(Pi, Qi, k, "stack_based", layout=layi, world_bounds=wbi), reps=1)
+    idsi = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    d2i = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    t = timed(lambda: ck.knn(Pi, Qi, k, "stack_based", layout=layi, world_bounds=wbi,
+                             out_ids=idsi, out_d2=d2i), reps=1)
     out["int3_knn64_queries_per_s"] = round(nq / (t / 1e3), 1)
     kb, mv = _knn_bytes(ck, Pi, Qi[:1_000_000], k, 12, 12, scale=nq // 1_000_000, layout=layi,
                         world_bounds=wbi)
     out["int3_knn64_frac"] = _frac(kb, t, peak)
-    out["int3_learned"] = "unavailable: the learned radius model is float3-only"
+    out["int3_learned"] = _learned_side_by_side(
+        ck, Pi, Qi, k, t, idsi, d2i, layi, wbi, len(pi),
+        torch.from_numpy(wl.int3_points(1_000_000, seed=11)).to(dev), num_dims=3, grid_res=64)
+    del idsi, d2i
     out["clocks"] = sampler.stop()
     try:
         from oracle import pyoracle as po

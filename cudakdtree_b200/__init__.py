@@ -183,6 +183,8 @@ def lib():
         L.cukd_spatial_knn.argtypes = [C.POINTER(SpatialTreeC), C.POINTER(Layout), P, I64,
                                        C.POINTER(QueryParams), P, P, P, P]
         L.cukd_radius_model_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_uint64]
+        L.cukd_radius_model_create_nd.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int,
+                                                  C.c_uint64]
         L.cukd_radius_model_destroy.argtypes = [C.c_void_p]
         L.cukd_radius_model_set_loss.argtypes = [C.c_void_p, C.c_float]
         L.cukd_radius_model_set_grid.argtypes = [C.c_void_p, P, I64, C.POINTER(Layout), P, P]
@@ -525,15 +527,17 @@ class RadiusModel:
     density -> 64 -> 64 -> 1, BF16 weights, trained on the GPU by the
     library's own kernels on exact k-th distances."""
 
-    NUM_PARAMS = 4545
+    NUM_PARAMS = 4801
+    NUM_INPUTS = 8
 
-    def __init__(self, grid_res=64, seed=0, quantile=0.0):
-        """quantile: 0 trains with mean squared error (the network predicts
-        the conditional mean of the log k-th distance); 0 < q < 1 with the
-        pinball loss (it predicts that quantile)."""
+    def __init__(self, grid_res=64, seed=0, quantile=0.0, num_dims=3):
+        """num_dims: dimension of the tree's points (2..4).  quantile: 0
+        trains with mean squared error (the network predicts the conditional
+        mean of the log k-th distance); 0 < q < 1 with the pinball loss (it
+        predicts that quantile)."""
         self.h = C.c_void_p()
-        _check(lib().cukd_radius_model_create(C.byref(self.h), grid_res, seed),
-               "cukd_radius_model_create")
+        _check(lib().cukd_radius_model_create_nd(C.byref(self.h), grid_res, num_dims, seed),
+               "cukd_radius_model_create_nd")
         _check(lib().cukd_radius_model_set_loss(self.h, float(quantile)),
                "cukd_radius_model_set_loss")
         self.final_loss = None
@@ -548,7 +552,8 @@ class RadiusModel:
 
     def set_grid(self, tree, layout, world_bounds, n=None, stream=None):
         n = _num_records(tree, layout) if n is None else n
-        wb = (C.c_float * 6)(*[float(v) for v in world_bounds.detach().cpu().reshape(-1)])
+        vals = [float(v) for v in world_bounds.detach().cpu().reshape(-1)]
+        wb = (C.c_float * len(vals))(*vals)
         _check(lib().cukd_radius_model_set_grid(self.h, _ptr(tree), n, C.byref(layout),
                                                 C.cast(wb, C.c_void_p), _stream(stream)),
                "cukd_radius_model_set_grid")
@@ -583,7 +588,8 @@ class RadiusModel:
         return r
 
     def features(self, queries, stream=None):
-        f = torch.empty((queries.shape[0], 4), dtype=torch.float32, device=queries.device)
+        f = torch.empty((queries.shape[0], self.NUM_INPUTS), dtype=torch.float32,
+                        device=queries.device)
         _check(lib().cukd_radius_model_features(self.h, _ptr(queries.contiguous()),
                                                 queries.shape[0], _ptr(f), _stream(stream)),
                "cukd_radius_model_features")
@@ -611,7 +617,8 @@ def knn_learned(tree, queries, k, model, method="stack_based", layout=None, worl
     nq = queries.shape[0]
     dev = queries.device
     ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32, device=dev)
-    d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=torch.float32, device=dev)
+    dt = torch.float32 if layout.scalar_type == FLOAT32 else torch.int64
+    d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, device=dev)
     fb = torch.zeros(2, dtype=torch.int32, device=dev)
     v = torch.zeros(nq, dtype=torch.int64, device=dev) if visits else None
     st = torch.zeros(nq, dtype=torch.int32, device=dev) if status else None

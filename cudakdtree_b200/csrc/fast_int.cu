@@ -47,7 +47,15 @@ __global__ void __launch_bounds__(256) knn_fast_int_kernel(FastArgs fa)
     const int32_t *qp = (const int32_t *)a.queries + myq * D;
 #pragma unroll
     for (int d = 0; d < D; d++) q[d] = __ldg(qp + d);
-    const long long r2 = a.cutoff_d2;
+    long long r2 = a.cutoff_d2;
+    if (fa.radius) {
+      // learned initial radius (any bound is exact: the answer is checked
+      // below; only the number of fallbacks depends on it)
+      const double rr = double(__ldg(fa.radius + myq)) * double(fa.radius_scale);
+      const double rb = ceil(rr * rr);
+      const long long seed = rb >= 9.0e18 ? 0x7fffffffffffffffll : (long long)rb;
+      r2 = seed < r2 ? seed : r2;
+    }
     for (int j = 0; j < K1; j++) {
       hd[j] = r2;
       hid[j] = 0xffffffffu;

@@ -57,27 +57,45 @@ struct ModelDev {
   float *params;          // FP32 master
   __nv_bfloat16 *wbf;     // BF16 copy used by every pass
   float *m, *v, *grad;    // Adam state, gradient accumulator
-  uint32_t *grid;         // res^3 counts
-  float *dens;            // res^3 log1pf(count): the density feature's cells
+  uint32_t *grid;         // res^D counts
+  float *dens;            // res^D log1pf(count): the density feature's cells
   float *loss;            // per-step loss sums
 };
 
+// a coordinate word of scalar type SC (0 float, 1 int32) as a float
+template <int SC> __device__ __forceinline__ float coord_f(uint32_t bits)
+{
+  return SC == 0 ? __uint_as_float(bits) : float(int32_t(bits));
+}
+
 // ---------------------------------------------------------------------------
+template <int D, int SC>
 __global__ void grid_count_kernel(const uint8_t *__restrict__ pts, int64_t n, int stride,
                                   int poff, Norm nm, uint32_t *grid)
 {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
-    const float *c = (const float *)(pts + i * stride + poff);
+    const uint32_t *c = (const uint32_t *)(pts + i * stride + poff);
     int cell = 0;
-    for (int d = 0; d < 3; d++) {
-      const float u = __fmul_rn(__fsub_rn(__ldg(c + d), nm.lo[d]), nm.invext[d]);
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const float x = coord_f<SC>(__ldg(c + d));
+      const float u = __fmul_rn(__fsub_rn(x, nm.lo[d]), nm.invext[d]);
       const float cc = __fmul_rn(u, float(nm.res));
       const int ci = cc >= 0.f ? (cc < float(nm.res) ? int(cc) : nm.res - 1) : 0;
       cell = cell * nm.res + ci;
     }
     atomicAdd(&grid[cell], 1u);
   }
+}
+
+// query i's coordinates (scalar type SC, D per query) as floats
+template <int D, int SC>
+__device__ __forceinline__ void query_f(const void *q, int64_t i, float *out)
+{
+  const uint32_t *w = (const uint32_t *)q + i * D;
+#pragma unroll
+  for (int d = 0; d < D; d++) out[d] = coord_f<SC>(__ldg(w + d));
 }
 
 __global__ void density_kernel(const uint32_t *grid, int64_t cells, float *dens)
@@ -97,24 +115,29 @@ __global__ void grid_max_kernel(const uint32_t *grid, int64_t cells, uint32_t *o
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-__global__ void features_kernel(const float *__restrict__ q, int64_t nq, Norm nm,
+template <int D, int SC>
+__global__ void features_kernel(const void *__restrict__ q, int64_t nq, Norm nm,
                                 const float *dens, float *feat)
 {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nq) return;
-  float qq[3] = {q[i * 3], q[i * 3 + 1], q[i * 3 + 2]};
-  float f[4];
-  features(nm, dens, qq, f);
+  float qq[D];
+  query_f<D, SC>(q, i, qq);
+  float f[kIn];
+  features<D>(nm, dens, qq, f);
 #pragma unroll
-  for (int d = 0; d < 4; d++) feat[i * 4 + d] = f[d];
+  for (int d = 0; d < kIn; d++) feat[i * kIn + d] = f[d];
 }
 
-// targets: standardised log of the k-th distance (from squared distances)
-__global__ void targets_kernel(const float *kth_d2, int64_t nq, float *t)
+// targets: standardised log of the k-th distance (from squared distances:
+// float for float trees, int64 for int trees)
+template <int SC>
+__global__ void targets_kernel(const void *kth_d2, int64_t nq, float *t)
 {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nq) return;
-  t[i] = __fmul_rn(0.5f, logf(fmaxf(kth_d2[i], 1e-30f)));
+  const float d2 = SC == 0 ? ((const float *)kth_d2)[i] : float(((const long long *)kth_d2)[i]);
+  t[i] = __fmul_rn(0.5f, logf(fmaxf(d2, 1e-30f)));
 }
 
 __global__ void normalize_targets_kernel(float *t, int64_t nq, float mean, float invstd)
@@ -128,8 +151,8 @@ __global__ void normalize_targets_kernel(float *t, int64_t nq, float mean, float
 // fused forward + backward over one slice of S samples per CTA
 // ---------------------------------------------------------------------------
 struct TrainSmem {
-  float w1[H][4], b1[H], w2[H][H], b2[H], w3[H], b3;
-  float f[S][4], h1[S][H], h2[S][H], dh2[S][H], dh1[S][H];
+  float w1[H][kIn], b1[H], w2[H][H], b2[H], w3[H], b3;
+  float f[S][kIn], h1[S][H], h2[S][H], dh2[S][H], dh1[S][H];
   float y[S], dy[S];
 };
 
@@ -145,7 +168,7 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
   const int tid = threadIdx.x;
   for (int i = tid; i < NP; i += kTrainThreads) {
     const float w = __bfloat162float(wbf[i]);
-    if (i < OB1) M.w1[(i - OW1) / 4][(i - OW1) % 4] = w;
+    if (i < OB1) M.w1[(i - OW1) / kIn][(i - OW1) % kIn] = w;
     else if (i < OW2) M.b1[i - OB1] = w;
     else if (i < OB2) M.w2[(i - OW2) / H][(i - OW2) % H] = w;
     else if (i < OW3) M.b2[i - OB2] = w;
@@ -155,9 +178,9 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
   const int64_t s0 = begin + int64_t(blockIdx.x) * S;
   const int64_t left = begin + count - s0;
   const int ns = left <= 0 ? 0 : (left < S ? int(left) : S);
-  for (int i = tid; i < S * 4; i += kTrainThreads) {
-    const int s = i / 4;
-    M.f[s][i % 4] = s < ns ? bf16_round(feat[(s0 + s) * 4 + i % 4]) : 0.f;
+  for (int i = tid; i < S * kIn; i += kTrainThreads) {
+    const int s = i / kIn;
+    M.f[s][i % kIn] = s < ns ? bf16_round(feat[(s0 + s) * kIn + i % kIn]) : 0.f;
   }
   __syncthreads();
   if (ns == 0) return;
@@ -166,7 +189,7 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
     const int s = i / H, j = i % H;
     float z = M.b1[j];
 #pragma unroll
-    for (int c = 0; c < 4; c++) z = __fmaf_rn(M.w1[j][c], M.f[s][c], z);
+    for (int c = 0; c < kIn; c++) z = __fmaf_rn(M.w1[j][c], M.f[s][c], z);
     M.h1[s][j] = bf16_round(fmaxf(z, 0.f));  // as the tensor cores see it
   }
   __syncthreads();
@@ -221,7 +244,7 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(
   for (int i = tid; i < NP; i += kTrainThreads) {
     float g = 0.f;
     if (i < OB1) {
-      const int j = (i - OW1) / 4, c = (i - OW1) % 4;
+      const int j = (i - OW1) / kIn, c = (i - OW1) % kIn;
       for (int s = 0; s < S; s++) g = __fmaf_rn(M.dh1[s][j], M.f[s][c], g);
     } else if (i < OW2) {
       const int j = i - OB1;
@@ -261,17 +284,19 @@ __global__ void adam_kernel(float *params, __nv_bfloat16 *wbf, float *m, float *
 // ---------------------------------------------------------------------------
 // inference: 32 queries per warp through mlp_forward_warp (tensor cores)
 // ---------------------------------------------------------------------------
+template <int D, int SC>
 __global__ void __launch_bounds__(128, 4) infer_kernel(const __nv_bfloat16 *__restrict__ wbf,
-                                                    const float *__restrict__ q, int64_t nq,
+                                                    const void *__restrict__ q, int64_t nq,
                                                     Norm nm, const float *dens, float *radius)
 {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i - (threadIdx.x & 31) >= nq) return;  // whole warps only: they run the mma together
   const bool live = i < nq;
   const int64_t qi = live ? i : 0;
-  const float qq[3] = {__ldg(q + qi * 3), __ldg(q + qi * 3 + 1), __ldg(q + qi * 3 + 2)};
-  float f[4];
-  features(nm, dens, qq, f);
+  float qq[D];
+  query_f<D, SC>(q, qi, qq);
+  float f[kIn];
+  features<D>(nm, dens, qq, f);
   const float y = mlp_forward_warp(wbf, f);
   if (live) radius[i] = expf(__fmaf_rn(y, nm.tstd, nm.tmean));
 }
@@ -284,7 +309,7 @@ __global__ void __launch_bounds__(128, 4) infer_kernel(const __nv_bfloat16 *__re
 // the network's instructions mostly fill issue slots the traversal leaves
 // idle.
 // ---------------------------------------------------------------------------
-template <bool EXPL, bool VEC16, int KC>
+template <int D, bool EXPL, bool VEC16, int KC>
 __global__ void __launch_bounds__(256, KC <= 17 ? 4 : 2)
     knn_learned_kernel(fast::FastArgs fa, const __nv_bfloat16 *__restrict__ wbf,
                        const float *__restrict__ dens, Norm nm)
@@ -298,18 +323,18 @@ __global__ void __launch_bounds__(256, KC <= 17 ? 4 : 2)
     const bool live = i < nq;
     // lanes past the end (last warp) predict query 0's radius and stop
     const int64_t myq = live ? (fa.q.order ? int64_t(__ldg(fa.q.order + i)) : i) : 0;
-    const float *qp = (const float *)fa.q.queries + myq * 3;
-    const float qq[3] = {__ldg(qp), __ldg(qp + 1), __ldg(qp + 2)};
-    float f[4];
-    features(nm, dens, qq, f);
+    float qq[D];
+    query_f<D, 0>(fa.q.queries, myq, qq);
+    float f[kIn];
+    features<D>(nm, dens, qq, f);
     __syncwarp();
     const float y = mlp_forward_warp(wbf, f);
     const float r = expf(__fmaf_rn(y, nm.tstd, nm.tmean));
-    if (live) fast::knn_fast_one<3, EXPL, VEC16, KC>(fa, i, myq, true, r);
+    if (live) fast::knn_fast_one<D, EXPL, VEC16, KC>(fa, i, myq, true, r);
   }
 }
 
-template <bool EXPL, bool VEC16>
+template <int D, bool EXPL, bool VEC16>
 int launch_learned(const fast::FastArgs &fa, const __nv_bfloat16 *wbf, const float *dens,
                    const Norm &nm, cudaStream_t st)
 {
@@ -317,21 +342,47 @@ int launch_learned(const fast::FastArgs &fa, const __nv_bfloat16 *wbf, const flo
   const unsigned grid = unsigned(std::max<int64_t>(1, div_up(fa.q.nq, bs)));
   const int slots = fa.kk + 1;
   if (slots <= 5)
-    knn_learned_kernel<EXPL, VEC16, 5><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+    knn_learned_kernel<D, EXPL, VEC16, 5><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
   else if (slots <= 9)
-    knn_learned_kernel<EXPL, VEC16, 9><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+    knn_learned_kernel<D, EXPL, VEC16, 9><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
   else if (slots <= 17)
-    knn_learned_kernel<EXPL, VEC16, 17><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+    knn_learned_kernel<D, EXPL, VEC16, 17><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
   else if (slots <= 33)
-    knn_learned_kernel<EXPL, VEC16, 33><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
+    knn_learned_kernel<D, EXPL, VEC16, 33><<<grid, bs, 0, st>>>(fa, wbf, dens, nm);
   else
     return CUKD_ERR_UNSUPPORTED;
   CKB_CHECK_LAUNCH();
   return CUKD_OK;
 }
 
-// deterministic initialisation (He-uniform), a 64-bit LCG seeded by the caller
-static void init_params(std::vector<float> &p, uint64_t seed)
+template <int D>
+int launch_learned_layout(const fast::FastArgs &fa, const Layout &L, const __nv_bfloat16 *wbf,
+                          const float *dens, const Norm &nm, cudaStream_t st)
+{
+  const bool expl = L.doff >= 0;
+  const bool vec16 = L.stride == 16 && L.poff == 0 && (!expl || L.doff == 12) && D <= 3;
+  if (expl)
+    return vec16 ? launch_learned<D, true, true>(fa, wbf, dens, nm, st)
+                 : launch_learned<D, true, false>(fa, wbf, dens, nm, st);
+  return vec16 ? launch_learned<D, false, true>(fa, wbf, dens, nm, st)
+               : launch_learned<D, false, false>(fa, wbf, dens, nm, st);
+}
+
+// (D, scalar) dispatch of the per-query model kernels
+#define CKB_MODEL_DISPATCH(D_, SC_, CALL)                          \
+  do {                                                            \
+    if ((D_) == 2 && (SC_) == 0) { constexpr int D = 2, SC = 0; CALL; } \
+    else if ((D_) == 3 && (SC_) == 0) { constexpr int D = 3, SC = 0; CALL; } \
+    else if ((D_) == 4 && (SC_) == 0) { constexpr int D = 4, SC = 0; CALL; } \
+    else if ((D_) == 2 && (SC_) == 1) { constexpr int D = 2, SC = 1; CALL; } \
+    else if ((D_) == 3 && (SC_) == 1) { constexpr int D = 3, SC = 1; CALL; } \
+    else if ((D_) == 4 && (SC_) == 1) { constexpr int D = 4, SC = 1; CALL; } \
+    else return CUKD_ERR_UNSUPPORTED;                             \
+  } while (0)
+
+// deterministic initialisation (He-uniform over the D + 1 real inputs), a
+// 64-bit LCG seeded by the caller
+static void init_params(std::vector<float> &p, uint64_t seed, int D)
 {
   uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
   auto uni = [&]() {
@@ -339,7 +390,7 @@ static void init_params(std::vector<float> &p, uint64_t seed)
     return float((x >> 11) * (1.0 / 9007199254740992.0)) * 2.f - 1.f;
   };
   p.assign(NP, 0.f);
-  for (int i = 0; i < 4 * H; i++) p[OW1 + i] = uni() * std::sqrt(6.f / 4.f);
+  for (int i = 0; i < kIn * H; i++) p[OW1 + i] = uni() * std::sqrt(6.f / float(D + 1));
   for (int i = 0; i < H * H; i++) p[OW2 + i] = uni() * std::sqrt(6.f / float(H));
   for (int i = 0; i < H; i++) p[OW3 + i] = uni() * std::sqrt(3.f / float(H));
 }
@@ -353,7 +404,7 @@ int run_fast(const fast::FastArgs &fa, int D, cudaStream_t st);
 // opaque model handle
 struct cukd_radius_model_s {
   int device;
-  int k;
+  int scalar;  // coordinate type of the tree the grid was built from
   ckb::learned::Norm norm;
   ckb::learned::ModelDev d;
   int trained;
@@ -364,35 +415,46 @@ struct cukd_radius_model_s {
 using namespace ckb;
 using namespace ckb::learned;
 
-static int model_alloc(cukd_radius_model_s *m, int res)
+static int64_t grid_cells(int res, int D)
+{
+  int64_t c = 1;
+  for (int d = 0; d < D; d++) c *= res;
+  return c;
+}
+
+static int model_alloc(cukd_radius_model_s *m, int64_t cells)
 {
   CKB_CUDA(cudaMalloc(&m->d.params, sizeof(float) * NP));
   CKB_CUDA(cudaMalloc(&m->d.wbf, sizeof(__nv_bfloat16) * NP));
   CKB_CUDA(cudaMalloc(&m->d.m, sizeof(float) * NP));
   CKB_CUDA(cudaMalloc(&m->d.v, sizeof(float) * NP));
   CKB_CUDA(cudaMalloc(&m->d.grad, sizeof(float) * NP));
-  CKB_CUDA(cudaMalloc(&m->d.grid, sizeof(uint32_t) * size_t(res) * res * res));
-  CKB_CUDA(cudaMalloc(&m->d.dens, sizeof(float) * size_t(res) * res * res));
+  CKB_CUDA(cudaMalloc(&m->d.grid, sizeof(uint32_t) * size_t(cells)));
+  CKB_CUDA(cudaMalloc(&m->d.dens, sizeof(float) * size_t(cells)));
   CKB_CUDA(cudaMalloc(&m->d.loss, sizeof(float) * 2));
   return CUKD_OK;
 }
 
 extern "C" {
 
-int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t seed)
+int cukd_radius_model_create_nd(cukd_radius_model **out, int grid_res, int num_dims,
+                                uint64_t seed)
 {
-  if (!out || grid_res < 1 || grid_res > 256) return CUKD_ERR_INVALID_ARGUMENT;
+  if (!out || num_dims < 2 || num_dims > 4 || grid_res < 1 ||
+      grid_cells(grid_res, num_dims) > (int64_t(1) << 24))
+    return CUKD_ERR_INVALID_ARGUMENT;
   auto *m = new cukd_radius_model_s();
   CKB_CUDA(cudaGetDevice(&m->device));
   m->norm.res = grid_res;
+  m->norm.D = num_dims;
   m->trained = 0;
-  const int rc = model_alloc(m, grid_res);
+  const int rc = model_alloc(m, grid_cells(grid_res, num_dims));
   if (rc != CUKD_OK) {
     cukd_radius_model_destroy((cukd_radius_model *)m);
     return rc;
   }
   std::vector<float> p;
-  init_params(p, seed);
+  init_params(p, seed, num_dims);
   std::vector<__nv_bfloat16> pb(NP);
   for (int i = 0; i < NP; i++) pb[i] = __float2bfloat16_rn(p[i]);
   CKB_CUDA(cudaMemcpy(m->d.params, p.data(), sizeof(float) * NP, cudaMemcpyHostToDevice));
@@ -402,6 +464,11 @@ int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t see
   CKB_CUDA(cudaMemset(m->d.grad, 0, sizeof(float) * NP));
   *out = (cukd_radius_model *)m;
   return CUKD_OK;
+}
+
+int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t seed)
+{
+  return cukd_radius_model_create_nd(out, grid_res, 3, seed);
 }
 
 int cukd_radius_model_set_loss(cukd_radius_model *model, float quantile)
@@ -425,27 +492,29 @@ int cukd_radius_model_destroy(cukd_radius_model *model)
   return CUKD_OK;
 }
 
-// Occupancy grid of the tree's points inside d_world_bounds (float3 trees).
+// Occupancy grid of the tree's points inside the world bounds.
 int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_points, int64_t n,
                                const cukd_layout *layout, const float *h_world_bounds,
                                cudaStream_t st)
 {
   auto *m = (cukd_radius_model_s *)model;
   ckb::Layout L;
-  if (!m || !make_layout(layout, &L) || L.scalar != CUKD_FLOAT32 || L.D != 3 ||
-      !h_world_bounds)
+  if (!m || !make_layout(layout, &L) || L.D != m->norm.D || !h_world_bounds)
     return CUKD_ERR_INVALID_ARGUMENT;
   Norm &nm = m->norm;
-  for (int d = 0; d < 3; d++) {
-    const float lo = h_world_bounds[d], hi = h_world_bounds[3 + d];
+  const int D = L.D;
+  m->scalar = L.scalar;
+  for (int d = 0; d < D; d++) {
+    const float lo = h_world_bounds[d], hi = h_world_bounds[D + d];
     nm.lo[d] = lo;
     nm.invext[d] = hi > lo ? 1.f / (hi - lo) : 0.f;
   }
-  const int64_t cells = int64_t(nm.res) * nm.res * nm.res;
+  const int64_t cells = grid_cells(nm.res, D);
   CKB_CUDA(cudaMemsetAsync(m->d.grid, 0, sizeof(uint32_t) * cells, st));
   const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(div_up(n, 256), kNumSMs * 8)));
-  grid_count_kernel<<<blocks, 256, 0, st>>>((const uint8_t *)d_points, n, L.stride, L.poff, nm,
-                                            m->d.grid);
+  CKB_MODEL_DISPATCH(D, L.scalar, (grid_count_kernel<D, SC><<<blocks, 256, 0, st>>>(
+                                      (const uint8_t *)d_points, n, L.stride, L.poff, nm,
+                                      m->d.grid)));
   CKB_CHECK_LAUNCH();
   uint32_t *mx = nullptr;
   CKB_CUDA(cudaMallocAsync(&mx, sizeof(uint32_t), st));
@@ -464,10 +533,30 @@ int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_points, i
   return CUKD_OK;
 }
 
+static int features_launch(const cukd_radius_model_s *m, const void *q, int64_t nq, float *feat,
+                           cudaStream_t st)
+{
+  const unsigned nb = unsigned(div_up(nq, 256));
+  CKB_MODEL_DISPATCH(m->norm.D, m->scalar, (features_kernel<D, SC><<<nb, 256, 0, st>>>(
+                                               q, nq, m->norm, m->d.dens, feat)));
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
+static int infer_launch(const cukd_radius_model_s *m, const void *q, int64_t nq, float *radius,
+                        cudaStream_t st)
+{
+  const unsigned nb = unsigned(div_up(nq, 128));
+  CKB_MODEL_DISPATCH(m->norm.D, m->scalar, (infer_kernel<D, SC><<<nb, 128, 0, st>>>(
+                                               m->d.wbf, q, nq, m->norm, m->d.dens, radius)));
+  CKB_CHECK_LAUNCH();
+  return CUKD_OK;
+}
+
 // Trains on (queries, exact k-th squared distances): standardises the log
 // distances, then `epochs` passes of Adam over minibatches of `batch`.
-int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
-                            const float *d_kth_d2, int64_t nq, int epochs, int batch, float lr,
+int cukd_radius_model_train(cukd_radius_model *model, const void *d_queries,
+                            const void *d_kth_d2, int64_t nq, int epochs, int batch, float lr,
                             float *h_final_loss, cudaStream_t st)
 {
   auto *m = (cukd_radius_model_s *)model;
@@ -475,12 +564,14 @@ int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
     return CUKD_ERR_INVALID_ARGUMENT;
   TempArena arena(st, nullptr);
   float *feat = nullptr, *tgt = nullptr;
-  CKB_TRY(arena.alloc(&feat, nq * 4));
+  CKB_TRY(arena.alloc(&feat, nq * kIn));
   CKB_TRY(arena.alloc(&tgt, nq));
   const unsigned nb = unsigned(div_up(nq, 256));
-  features_kernel<<<nb, 256, 0, st>>>(d_queries, nq, m->norm, m->d.dens, feat);
-  CKB_CHECK_LAUNCH();
-  targets_kernel<<<nb, 256, 0, st>>>(d_kth_d2, nq, tgt);
+  CKB_TRY(features_launch(m, d_queries, nq, feat, st));
+  if (m->scalar == CUKD_FLOAT32)
+    targets_kernel<0><<<nb, 256, 0, st>>>(d_kth_d2, nq, tgt);
+  else
+    targets_kernel<1><<<nb, 256, 0, st>>>(d_kth_d2, nq, tgt);
   CKB_CHECK_LAUNCH();
   // standardise targets (host statistics; one read of nq floats)
   std::vector<float> ht(nq);
@@ -527,16 +618,13 @@ int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
 }
 
 // Per-query predicted k-th-neighbour distance (before the safety scale).
-int cukd_radius_model_predict(const cukd_radius_model *model, const float *d_queries, int64_t nq,
+int cukd_radius_model_predict(const cukd_radius_model *model, const void *d_queries, int64_t nq,
                               float *d_out_radius, cudaStream_t st)
 {
   auto *m = (const cukd_radius_model_s *)model;
   if (!m || (nq > 0 && (!d_queries || !d_out_radius))) return CUKD_ERR_INVALID_ARGUMENT;
   if (nq == 0) return CUKD_OK;
-  infer_kernel<<<unsigned(div_up(nq, 128)), 128, 0, st>>>(m->d.wbf, d_queries, nq, m->norm,
-                                                          m->d.dens, d_out_radius);
-  CKB_CHECK_LAUNCH();
-  return CUKD_OK;
+  return infer_launch(m, d_queries, nq, d_out_radius, st);
 }
 
 // Gradient of the mean squared error over one batch of (features, standardised
@@ -573,16 +661,13 @@ int cukd_radius_model_gradients(cukd_radius_model *model, const float *d_feature
 }
 
 // Features of a batch of queries (the model's input), for inspection/tests.
-int cukd_radius_model_features(const cukd_radius_model *model, const float *d_queries,
+int cukd_radius_model_features(const cukd_radius_model *model, const void *d_queries,
                                int64_t nq, float *d_out_features, cudaStream_t st)
 {
   auto *m = (const cukd_radius_model_s *)model;
   if (!m || nq < 0) return CUKD_ERR_INVALID_ARGUMENT;
   if (nq == 0) return CUKD_OK;
-  features_kernel<<<unsigned(div_up(nq, 256)), 256, 0, st>>>(d_queries, nq, m->norm, m->d.dens,
-                                                              d_out_features);
-  CKB_CHECK_LAUNCH();
-  return CUKD_OK;
+  return features_launch(m, d_queries, nq, d_out_features, st);
 }
 
 // kNN with the learned radius: same results as cukd_knn (plain), see the
@@ -599,9 +684,9 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
 {
   auto *m = (const cukd_radius_model_s *)model;
   ckb::Layout L;
-  if (!m || !p || !make_layout(layout, &L) || L.scalar != CUKD_FLOAT32 || L.D != 3)
+  if (!m || !p || !make_layout(layout, &L) || L.D != m->norm.D || L.scalar != m->scalar)
     return CUKD_ERR_INVALID_ARGUMENT;
-  if (p->k < 2 || p->k > 32 || (p->flags & CUKD_QUERY_HEAP_ORDER) || radius_scale <= 0.f)
+  if (p->k < 2 || p->k > 128 || (p->flags & CUKD_QUERY_HEAP_ORDER) || radius_scale <= 0.f)
     return CUKD_ERR_UNSUPPORTED;
   if (nq == 0) return CUKD_OK;
   if (!d_queries || !d_out_ids || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;
@@ -625,10 +710,11 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   a.out_d2 = d_out_d2;
   a.visits = d_visits;
   a.block_size = p->block_size;
-  if ((p->flags & CUKD_QUERY_MORTON) && nq > 1) {
+  if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32) {
     int32_t *perm = nullptr;
     CKB_TRY(arena.alloc(&perm, nq));
-    CKB_TRY(cukd_morton_order((const float *)d_queries, nq, 3, nullptr, perm, st, mem));
+    CKB_TRY(cukd_morton_order((const float *)d_queries, nq, L.D, (const float *)d_world_bounds,
+                              perm, st, mem));
     a.order = perm;
   }
   int *ctr = nullptr;
@@ -637,7 +723,6 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   int32_t *fb1 = nullptr, *fb2 = nullptr;
   CKB_TRY(arena.alloc(&fb1, nq));
   CKB_TRY(arena.alloc(&fb2, nq));
-  // pass 1: radii predicted and searched in one kernel
   fast::FastArgs fa = {};
   fa.q = a;
   fa.kk = p->k;
@@ -646,32 +731,42 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   fa.fb_list = fb1;
   fa.radius_scale = radius_scale;
   fa.status = d_status;
-  {
-    const bool expl = L.doff >= 0;
-    const bool vec16 = L.stride == 16 && L.poff == 0 && (!expl || L.doff == 12);
-    const int rc = expl ? (vec16 ? launch_learned<true, true>(fa, m->d.wbf, m->d.dens, m->norm, st)
-                                 : launch_learned<true, false>(fa, m->d.wbf, m->d.dens, m->norm, st))
-                        : (vec16 ? launch_learned<false, true>(fa, m->d.wbf, m->d.dens, m->norm, st)
-                                 : launch_learned<false, false>(fa, m->d.wbf, m->d.dens, m->norm, st));
+  const bool isFloat = L.scalar == CUKD_FLOAT32;
+  if (isFloat && p->k <= 32) {
+    // pass 1: radii predicted and searched in one kernel
+    const int D = L.D;
+    const int rc = D == 2 ? launch_learned_layout<2>(fa, L, m->d.wbf, m->d.dens, m->norm, st)
+                 : D == 3 ? launch_learned_layout<3>(fa, L, m->d.wbf, m->d.dens, m->norm, st)
+                          : launch_learned_layout<4>(fa, L, m->d.wbf, m->d.dens, m->norm, st);
     CKB_TRY(rc);
+  } else {
+    // pass 1: the radii predicted for every query, then the seeded traversal
+    // (the local-memory heap for k > 32, or the integer kernel)
+    float *radius = nullptr;
+    CKB_TRY(arena.alloc(&radius, nq));
+    CKB_TRY(infer_launch(m, d_queries, nq, radius, st));
+    fa.radius = radius;
+    CKB_TRY(isFloat ? run_fast(fa, L.D, st) : run_fast_int(fa, L.D, st));
   }
   // pass 2: plain unbounded traversal of the queries pass 1 could not answer
   fast::FastArgs fb = fa;
+  fb.radius = nullptr;
   fb.status = nullptr;
   fb.q.order = fb1;
   fb.q.count_ptr = ctr + 1;
   fb.fb_count = ctr + 2;
   fb.fb_list = fb2;
-  CKB_TRY(run_fast(fb, 3, st));
+  CKB_TRY(isFloat ? run_fast(fb, L.D, st) : run_fast_int(fb, L.D, st));
   // pass 3: boundary ties in the reference's visiting order
   query::QArgs c = a;
   c.order = fb2;
   c.count_ptr = ctr + 2;
   c.visits = nullptr;
-  const int kind = p->k <= 4 ? query::RES_FIX4
+  const int kind = p->k > 32 ? query::RES_HEAP128
+                 : p->k <= 4 ? query::RES_FIX4
                              : (p->k <= 8 ? query::RES_FIX8
                                           : (p->k <= 16 ? query::RES_FIX16 : query::RES_FIX32));
-  CKB_TRY(query::run_query(c, CUKD_FLOAT32, 3, p->method, kind, st));
+  CKB_TRY(query::run_query(c, L.scalar, L.D, p->method, kind, st));
   if (d_out_fallback)
     CKB_CUDA(cudaMemcpyAsync(d_out_fallback, ctr + 1, 2 * sizeof(int), cudaMemcpyDeviceToDevice,
                              st));

@@ -13,32 +13,41 @@ namespace ckb {
 namespace learned {
 
 constexpr int H = 64;
-constexpr int OW1 = 0;            // [H][4]  W1[j][i]
-constexpr int OB1 = OW1 + 4 * H;  // [H]
-constexpr int OW2 = OB1 + H;      // [H][H]  W2[j][k]: output j, input k
-constexpr int OB2 = OW2 + H * H;  // [H]
-constexpr int OW3 = OB2 + H;      // [H]
-constexpr int OB3 = OW3 + H;      // [1]
-constexpr int NP = OB3 + 1;       // 4545 parameters
+// network input: the query's D normalised coordinates (D = 2..4), its
+// density feature, zeros up to kIn (the first layer's input is padded to 8,
+// one k-pair per lane group of the tensor-core fragment)
+constexpr int kIn = 8;
+constexpr int OW1 = 0;              // [H][kIn]  W1[j][i]
+constexpr int OB1 = OW1 + kIn * H;  // [H]
+constexpr int OW2 = OB1 + H;        // [H][H]  W2[j][k]: output j, input k
+constexpr int OB2 = OW2 + H * H;    // [H]
+constexpr int OW3 = OB2 + H;        // [H]
+constexpr int OB3 = OW3 + H;        // [1]
+constexpr int NP = OB3 + 1;         // 4801 parameters
 // every block the forward pass reads as bf16 pairs starts on an even index
 static_assert(OB1 % 2 == 0 && OW2 % 2 == 0 && OB2 % 2 == 0 && OW3 % 2 == 0, "pair alignment");
 
 struct Norm {
-  float lo[3], invext[3];
-  int res;
-  float invLogMax;  // 1 / log(1 + max cell count)
-  float tmean, tstd;
+  float lo[4], invext[4];  // world box: coordinates -> [0, 1]
+  int D;                   // dimensions of the tree's points
+  int res;                 // grid cells per dimension (res^D cells)
+  float invLogMax;         // 1 / log(1 + max cell count)
+  float tmean, tstd;       // standardisation of the log k-th distance
 };
 
-// log(1 + cell count), trilinearly interpolated between the centres of the
-// 8 cells around the query (a smooth density estimate at grid scale);
-// `dens` holds log1pf(count) per cell, computed once per grid
+// Features of one query (coordinates already as floats): f[0..D) the
+// coordinates mapped to [-1, 1] over the world box, f[D] log(1 + cell count)
+// interpolated multilinearly between the centres of the 2^D cells around the
+// query (a smooth density estimate at grid scale), the rest 0.  `dens` holds
+// log1pf(count) per cell, computed once per grid; cells are row-major with
+// dimension 0 the slowest.
+template <int D>
 __device__ inline void features(const Norm &nm, const float *dens, const float *q, float *f)
 {
-  int c0[3];
-  float w[3];
+  int c0[D];
+  float w[D];
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
+  for (int d = 0; d < D; d++) {
     const float u = __fmul_rn(__fsub_rn(q[d], nm.lo[d]), nm.invext[d]);
     f[d] = __fsub_rn(__fmul_rn(u, 2.f), 1.f);
     // position in cell-centre coordinates
@@ -51,11 +60,11 @@ __device__ inline void features(const Norm &nm, const float *dens, const float *
   }
   float acc = 0.f;
 #pragma unroll
-  for (int corner = 0; corner < 8; corner++) {
+  for (int corner = 0; corner < (1 << D); corner++) {
     int cell = 0;
     float wt = 1.f;
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
+    for (int d = 0; d < D; d++) {
       const int bit = (corner >> d) & 1;
       const int ci = min(c0[d] + bit, nm.res - 1);
       cell = cell * nm.res + ci;
@@ -63,7 +72,9 @@ __device__ inline void features(const Norm &nm, const float *dens, const float *
     }
     acc = __fmaf_rn(wt, __ldg(dens + cell), acc);
   }
-  f[3] = __fmul_rn(acc, nm.invLogMax);
+  f[D] = __fmul_rn(acc, nm.invLogMax);
+#pragma unroll
+  for (int d = D + 1; d < kIn; d++) f[d] = 0.f;
 }
 
 // bf16 rounding of an activation as the tensor-core operands see it
@@ -97,7 +108,7 @@ __device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4],
 }
 
 // Forward pass of 32 queries on the tensor cores, one query per lane (all
-// 32 lanes must take part).  `f` holds this lane's 4 features; returns the
+// 32 lanes must take part).  `f` holds this lane's kIn features; returns the
 // standardised network output of this lane's query.
 //
 // Rows of the 32x64 activation tile are the lanes: m-tile 0 = lanes 0..15,
@@ -109,16 +120,18 @@ __device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4],
 // layer: activations never leave registers.  Inputs and hidden activations
 // enter the tensor cores as bf16 (the training forward pass rounds them
 // the same way); every product is accumulated in FP32.
-//   layer 1: [32 x 16 (4 features, zero padded)] x W1^T: 2 x 8 mma
+//   layer 1: [32 x 16 (8 inputs, zero padded)] x W1^T:  2 x 8 mma
 //   layer 2: [32 x 64] x W2^T:                           2 x 8 x 4 mma
 //   layer 3: 64-wide dot per row on the FP32 cores, reduced over the 4
 //            lanes that share a row
 __device__ __forceinline__ float mlp_forward_warp(const __nv_bfloat16 *__restrict__ w,
-                                                  const float f[4])
+                                                  const float f[kIn])
 {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const uint32_t p01 = pack_bf16x2(f[0], f[1]), p23 = pack_bf16x2(f[2], f[3]);
+  // this lane's input pair for column pair t of the A fragment
+  const uint32_t pair[4] = {pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                            pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7])};
   const float b3 = __bfloat162float(w[OB3]);
   float y00 = 0.f, y01 = 0.f, y10 = 0.f, y11 = 0.f;  // [m-tile][row g / g+8]
   // rolled loops over m-tiles and layer-2 n-tiles keep one accumulator tile
@@ -126,17 +139,23 @@ __device__ __forceinline__ float mlp_forward_warp(const __nv_bfloat16 *__restric
 #pragma unroll 1
   for (int mt = 0; mt < 2; mt++) {
     const int r0 = 16 * mt + g;
-    const uint32_t s0a = __shfl_sync(full, p01, r0), s0b = __shfl_sync(full, p23, r0);
-    const uint32_t s1a = __shfl_sync(full, p01, r0 + 8), s1b = __shfl_sync(full, p23, r0 + 8);
-    const uint32_t a1[4] = {t == 0 ? s0a : (t == 1 ? s0b : 0u), t == 0 ? s1a : (t == 1 ? s1b : 0u),
-                            0u, 0u};
+    // A fragment: rows r0 and r0 + 8, columns 2t and 2t+1 (inputs); columns
+    // 8..15 are zero padding
+    uint32_t s0 = 0u, s1 = 0u;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t v0 = __shfl_sync(full, pair[j], r0), v1 = __shfl_sync(full, pair[j], r0 + 8);
+      s0 = t == j ? v0 : s0;
+      s1 = t == j ? v1 : s1;
+    }
+    const uint32_t a1[4] = {s0, s1, 0u, 0u};
     uint32_t h1[4][4];  // A fragments of layer 2, one per k-tile
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
       const int col = 8 * nt + 2 * t;
       const float2 bb = ld_bf16x2(w, OB1 + col);
       float c[4] = {bb.x, bb.y, bb.x, bb.y};
-      const uint32_t b0 = t < 2 ? ld_u32(w, OW1 + 4 * (8 * nt + g) + 2 * t) : 0u;
+      const uint32_t b0 = ld_u32(w, OW1 + kIn * (8 * nt + g) + 2 * t);
       mma_16816(c, a1, b0, 0u);
       const uint32_t lo = pack_bf16x2(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
       const uint32_t hi = pack_bf16x2(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));

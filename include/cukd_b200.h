@@ -348,22 +348,30 @@ CUKD_API int cukd_spatial_knn(const cukd_spatial_tree *tree, const cukd_layout *
 /* ------------------------------------------------------------------------
  * Learned kNN-radius proposal (no reference counterpart)
  *
- * A small MLP (xyz + log density of a res^3 occupancy grid -> 64 -> 64 -> 1,
- * BF16 weights, FP32 accumulation) predicts each query's k-th-neighbour
- * distance.  cukd_knn_learned seeds every query's cull radius with the
- * prediction times a safety scale; queries that find fewer than k points
- * inside it (or hit an exact distance tie at the k-th boundary) are re-run
- * by the plain traversal, so its results equal cukd_knn's bit for bit.
- * float3 trees only.
+ * A small MLP (the query's D coordinates + log density of a res^D occupancy
+ * grid, padded to 8 inputs -> 64 -> 64 -> 1, BF16 weights and activations,
+ * FP32 accumulation, run on the tensor cores) predicts each query's k-th-
+ * neighbour distance.  cukd_knn_learned seeds every query's cull radius with
+ * the prediction times a safety scale; queries that find fewer than k
+ * points inside it (or hit an exact distance tie at the k-th boundary) are
+ * re-run by the plain traversal, so its results equal cukd_knn's bit for
+ * bit.  Trees of float or int32 points, D = 2..4 (a model is made for one
+ * D and learns on one coordinate type).
  * ------------------------------------------------------------------------ */
 typedef struct cukd_radius_model_s cukd_radius_model;
 
-/* Creates an untrained model (seeded initialisation) on the current device. */
+/* Creates an untrained model for num_dims-dimensional points (2..4; at most
+ * 2^24 grid cells) with a seeded initialisation on the current device. */
+CUKD_API int cukd_radius_model_create_nd(cukd_radius_model **out, int grid_res, int num_dims,
+                                         uint64_t seed);
+/* The same for 3-D points. */
 CUKD_API int cukd_radius_model_create(cukd_radius_model **out, int grid_res, uint64_t seed);
 CUKD_API int cukd_radius_model_destroy(cukd_radius_model *model);
 
 /* Builds the occupancy grid from the tree's points inside the world bounds
- * (h_world_bounds: host float[6], lower xyz then upper xyz). */
+ * (h_world_bounds: host float[2 * D], lower then upper; int trees pass their
+ * bounds as floats).  The layout's D must be the model's; its coordinate
+ * type becomes the type of the queries the model takes. */
 CUKD_API int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_points,
                                         int64_t n, const cukd_layout *layout,
                                         const float *h_world_bounds, cudaStream_t stream);
@@ -376,35 +384,39 @@ CUKD_API int cukd_radius_model_set_grid(cukd_radius_model *model, const void *d_
  * fallbacks to the plain traversal at the same radius scale. */
 CUKD_API int cukd_radius_model_set_loss(cukd_radius_model *model, float quantile);
 
-/* Trains on nq queries and their exact k-th squared distances (for example
- * the knn() return values of cukd_knn): Adam on minibatches, `epochs`
- * passes; *h_final_loss receives the last epoch's mean squared error on the
- * standardised log distance (or the pinball loss, cukd_radius_model_set_loss). */
-CUKD_API int cukd_radius_model_train(cukd_radius_model *model, const float *d_queries,
-                                     const float *d_kth_d2, int64_t nq, int epochs, int batch,
+/* Trains on nq queries (device point_t[nq] of the grid's coordinate type)
+ * and their exact k-th squared distances (float[nq] for float trees,
+ * int64[nq] for int trees; for example the knn() return values of
+ * cukd_knn): Adam on minibatches, `epochs` passes; *h_final_loss receives
+ * the last epoch's mean squared error on the standardised log distance (or
+ * the pinball loss, cukd_radius_model_set_loss). */
+CUKD_API int cukd_radius_model_train(cukd_radius_model *model, const void *d_queries,
+                                     const void *d_kth_d2, int64_t nq, int epochs, int batch,
                                      float lr, float *h_final_loss, cudaStream_t stream);
 
 /* Predicted k-th-neighbour distance per query (not squared, not scaled). */
-CUKD_API int cukd_radius_model_predict(const cukd_radius_model *model, const float *d_queries,
+CUKD_API int cukd_radius_model_predict(const cukd_radius_model *model, const void *d_queries,
                                        int64_t nq, float *d_out_radius, cudaStream_t stream);
 
-/* The model's 4 input features per query (device float[nq][4]). */
-CUKD_API int cukd_radius_model_features(const cukd_radius_model *model, const float *d_queries,
+/* The model's 8 input features per query (device float[nq][8]: D
+ * coordinates in [-1, 1], the density feature, zeros). */
+CUKD_API int cukd_radius_model_features(const cukd_radius_model *model, const void *d_queries,
                                         int64_t nq, float *d_out_features, cudaStream_t stream);
 
-/* Mean-squared-error gradient over n (features, standardised target) pairs
- * at the model's current BF16 weights, without updating them; also returns
- * those weights as floats and the loss (host buffers of 4545 floats).  For
+/* Loss gradient over n (features [n][8], standardised target) pairs at the
+ * model's current BF16 weights, without updating them; also returns those
+ * weights as floats and the loss (host buffers of 4801 floats).  For
  * checking the hand-written backward pass against a CPU oracle. */
 CUKD_API int cukd_radius_model_gradients(cukd_radius_model *model, const float *d_features,
                                          const float *d_targets, int64_t n, float *h_grad,
                                          float *h_params_bf16, float *h_loss,
                                          cudaStream_t stream);
 
-/* kNN (k = 2..32) seeded with the learned radius times radius_scale: the
- * queries are put in Morton order, the network predicts their radii in that
- * order on the tensor cores, and the candidate-list traversal starts each
- * query's cull radius at its prediction.
+/* kNN (k = 2..128) seeded with the learned radius times radius_scale: the
+ * queries are put in Morton order (float trees), the network predicts their
+ * radii on the tensor cores -- inside the search kernel for float trees and
+ * k <= 32, in a pass of its own otherwise -- and the fast traversal starts
+ * each query's cull radius at its prediction.
  * d_out_fallback (optional, device int[2]): queries re-run by the plain
  * traversal, and by the reference's own visiting order.  d_status
  * (optional, device int[nq]): 0 if the learned pass answered the query, 1 if

@@ -2,10 +2,11 @@
 
 Restates, in float64 numpy, the forward pass and the backward pass of the
 network that cudakdtree_b200/csrc/learned.cu trains:
-    f (4) -> 64 ReLU -> 64 ReLU -> 1,  loss = mean((y - t)^2)
+    f (8) -> 64 ReLU -> 64 ReLU -> 1,  loss = mean((y - t)^2) or pinball
 with the parameter vector laid out as
-    W1[64][4], b1[64], W2[64][64] (W2[j][k]: output j, input k), b2[64],
-    w3[64], b3.
+    W1[64][8], b1[64], W2[64][64] (W2[j][k]: output j, input k), b2[64],
+    w3[64], b3
+(8 inputs: the query's D coordinates, its density feature, zeros).
 The GPU computes in FP32 over BF16-rounded weights; the oracle is given
 those same rounded weights.  The inputs and the first hidden layer enter the
 GPU's products (tensor-core operands) as bf16, so the oracle rounds them the
@@ -15,7 +16,8 @@ accumulation rounding.
 import numpy as np
 
 H = 64
-OW1, OB1 = 0, 4 * H
+NIN = 8
+OW1, OB1 = 0, NIN * H
 OW2 = OB1 + H
 OB2 = OW2 + H * H
 OW3 = OB2 + H
@@ -25,7 +27,7 @@ NP = OB3 + 1
 
 def unpack(p):
     p = np.asarray(p, np.float64)
-    return (p[OW1:OB1].reshape(H, 4), p[OB1:OW2], p[OW2:OB2].reshape(H, H), p[OB2:OW3],
+    return (p[OW1:OB1].reshape(H, NIN), p[OB1:OW2], p[OW2:OB2].reshape(H, H), p[OB2:OW3],
             p[OW3:OB3], p[OB3])
 
 

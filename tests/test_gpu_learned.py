@@ -168,3 +168,69 @@ def test_trained_network_predicts_the_kth_distance():
     li, ld, fb, _ = ck.knn_learned(rec, q, 16, trained, layout=LAYOUT, world_bounds=wb)
     assert torch.equal(li, pi) and torch.equal(ld, pd)
     assert int(fb[0]) < 0.2 * q.shape[0]
+
+
+F4_RECORD = np.dtype({"names": ["p", "dim"], "formats": [(np.float32, (4,)), np.int32],
+                      "offsets": [0, 16], "itemsize": 32})
+F4_LAYOUT = ck.layout_for("float32", 4, stride=32, dim_offset=16, dim_bits=32)
+
+
+@pytest.mark.parametrize("k", [16, 64])
+def test_learned_float4_wide_records_identical_to_plain(k):
+    """Config 5's float part: {float4; int dim} records (the reference's
+    32-byte layout) with widest-extent dims; a 4-D model (4 coordinates +
+    a 4-D grid density) seeds the fused kernel (k = 16) or the heap kernel
+    (k = 64); answers equal the plain path's and the reference order's."""
+    n = 200000
+    pts = wl.wide_float4(n, seed=7)
+    rec = np.zeros(n, F4_RECORD)
+    rec["p"] = pts
+    d = torch.from_numpy(rec.view(np.uint8)).cuda()
+    wb = ck.build_tree(d, layout=F4_LAYOUT)
+    m = ck.RadiusModel(grid_res=16, seed=3, quantile=0.9, num_dims=4)
+    m.fit(d, torch.from_numpy(wl.wide_float4(40000, seed=8)).cuda(), k, layout=F4_LAYOUT,
+          world_bounds=wb, epochs=5)
+    q = torch.from_numpy(wl.wide_float4(30000, seed=9)).cuda()
+    pi, pd = ck.knn(d, q, k, layout=F4_LAYOUT, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(d, q, k, m, layout=F4_LAYOUT, world_bounds=wb)
+    assert torch.equal(li, pi)
+    assert np.array_equal(f32_bits(ld.cpu().numpy()), f32_bits(pd.cpu().numpy()))
+    ri, rd = ck.knn(d, q, k, layout=F4_LAYOUT, world_bounds=wb, reference_order=True)
+    assert torch.equal(li, ri)
+    assert int(fb[0]) < 0.3 * q.shape[0]
+
+
+@pytest.mark.parametrize("k", [8, 64])
+def test_learned_int3_identical_to_plain(k):
+    """Config 5's integer part: int3 points in [-2^20, 2^20]^3, exact int64
+    distances; the model learns on integer queries and seeds the integer
+    kernel with a radius rounded to an int64 bound."""
+    n = 300000
+    pts = wl.int3_points(n)
+    d = torch.from_numpy(pts).cuda()
+    wb = ck.build_tree(d)
+    m = ck.RadiusModel(grid_res=32, seed=4, quantile=0.9)
+    m.fit(d, torch.from_numpy(wl.int3_points(50000, seed=11)).cuda(), k, world_bounds=wb,
+          epochs=5)
+    q = torch.from_numpy(wl.int3_points(40000, seed=12)).cuda()
+    pi, pd = ck.knn(d, q, k, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(d, q, k, m, world_bounds=wb)
+    assert torch.equal(li, pi) and torch.equal(ld, pd)
+    ri, rd = ck.knn(d, q, k, world_bounds=wb, reference_order=True)
+    assert torch.equal(li, ri) and torch.equal(ld, rd)
+    assert int(fb[0]) < 0.3 * q.shape[0]
+
+
+def test_learned_float2_fused_identical_to_plain():
+    n = 300000
+    pts = wl.uniform_points(n, D=2, seed=21)
+    d = torch.from_numpy(pts).cuda()
+    wb = ck.build_tree(d)
+    m = ck.RadiusModel(grid_res=128, seed=5, num_dims=2)
+    m.fit(d, torch.from_numpy(wl.uniform_points(50000, D=2, seed=22)).cuda(), 16,
+          world_bounds=wb, epochs=5)
+    q = torch.from_numpy(wl.uniform_points(50000, D=2, seed=23)).cuda()
+    pi, pd = ck.knn(d, q, 16, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(d, q, 16, m, world_bounds=wb)
+    assert torch.equal(li, pi)
+    assert np.array_equal(f32_bits(ld.cpu().numpy()), f32_bits(pd.cpu().numpy()))

@@ -217,7 +217,7 @@ def test_mlp_oracle_gradient_matches_finite_differences():
     from oracle import mlp_oracle as mo
     rng = np.random.default_rng(0)
     p = rng.normal(0, 0.3, mo.NP)
-    f = rng.normal(0, 1, (16, 4))
+    f = rng.normal(0, 1, (16, mo.NIN))
     t = rng.normal(0, 1, 16)
     _, g = mo.loss_and_grad(p, f, t, bf16_act=False)
     for i in [0, 5, mo.OB1 + 3, mo.OW2 + 100, mo.OW2 + 4000, mo.OB2 + 7, mo.OW3 + 9, mo.OB3]:
@@ -236,7 +236,7 @@ def test_mlp_oracle_pinball_gradient_matches_finite_differences(quantile):
     from oracle import mlp_oracle as mo
     rng = np.random.default_rng(1)
     p = rng.normal(0, 0.3, mo.NP)
-    f = rng.normal(0, 1, (16, 4))
+    f = rng.normal(0, 1, (16, mo.NIN))
     y, _ = mo.forward(p, f, bf16_act=False)
     t = y + rng.choice([-1.0, 1.0], 16) * rng.uniform(0.1, 1.0, 16)
     _, g = mo.loss_and_grad(p, f, t, bf16_act=False, quantile=quantile)
