@@ -43,6 +43,7 @@ METHODS = {"stack_based": STACK_BASED, "stackBased": STACK_BASED, "stack_free": 
 BUILDERS = {"default": 0, "thrust": 1, "bitonic": 2, "inplace": 3, "inPlace": 3}
 QUERY_MORTON, QUERY_HEAP_ORDER, QUERY_FORCE_HEAP, QUERY_REFERENCE_ORDER = 1, 2, 4, 8
 QUERY_TREE_ORDER = 16
+QUERY_WARP_PACKET = 32
 INT64_MAX = (1 << 63) - 1
 ASYNC_WAIT_POLLS_DEFAULT = 4194304  # CUKD_ASYNC_WAIT_POLLS_DEFAULT
 
@@ -290,7 +291,7 @@ def build_tree(points, layout=None, world_bounds=None, builder="default", stream
 
 def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=True,
             heap_order=False, force_heap=False, block_size=0, reference_order=False,
-            tree_order=False):
+            tree_order=False, warp_packet=False):
     p = QueryParams()
     p.method = METHODS[method] if isinstance(method, str) else int(method)
     p.k = k
@@ -300,7 +301,8 @@ def _params(method, k=1, cutoff=math.inf, eps=0.0, cutoff_d2=INT64_MAX, morton=T
     p.flags = ((QUERY_MORTON if morton else 0) | (QUERY_HEAP_ORDER if heap_order else 0)
                | (QUERY_FORCE_HEAP if force_heap else 0)
                | (QUERY_REFERENCE_ORDER if reference_order else 0)
-               | (QUERY_TREE_ORDER if tree_order else 0))
+               | (QUERY_TREE_ORDER if tree_order else 0)
+               | (QUERY_WARP_PACKET if warp_packet else 0))
     p.block_size = block_size
     return p
 
@@ -330,9 +332,11 @@ def fcp(tree, queries, method="stack_based", layout=None, world_bounds=None, n=N
 def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
         cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, heap_order=False,
         force_heap=False, with_max=False, stream=None, block_size=0, out_ids=None,
-        out_d2=None, reference_order=False, reordered_count=None, tree_order=False):
+        out_d2=None, reference_order=False, reordered_count=None, tree_order=False,
+        warp_packet=False):
     """k nearest neighbours.  Returns (ids [nq,k] int32, d2 [nq,k]) with the
-    reference's candidate-list semantics; ascending unless heap_order."""
+    reference's candidate-list semantics; ascending unless heap_order.
+    warp_packet: the warp-cooperative traversal (float, k <= 32)."""
     layout = layout or infer_layout(tree)
     if n is None:
         n = _num_records(tree, layout)
@@ -343,7 +347,7 @@ def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, 
     d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, device=dev)
     mx = torch.empty(nq, dtype=dt, device=dev) if with_max else None
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton, heap_order, force_heap, block_size,
-                reference_order, tree_order)
+                reference_order, tree_order, warp_packet)
     if reordered_count is not None:  # int32 CUDA tensor of one element
         p.d_reordered_count = reordered_count.data_ptr()
     _check(lib().cukd_knn(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
@@ -609,9 +613,10 @@ class RadiusModel:
 
 def knn_learned(tree, queries, k, model, method="stack_based", layout=None, world_bounds=None,
                 n=None, scale=1.2, morton=True, visits=False, status=False, stream=None,
-                out_ids=None, out_d2=None):
+                out_ids=None, out_d2=None, warp_packet=False):
     """kNN seeded by the learned radius: same results as knn().  Returns
-    (ids, d2, fallback[2] int32 tensor, visits or None[, status])."""
+    (ids, d2, fallback[2] int32 tensor, visits or None[, status]).
+    warp_packet: seed the warp-cooperative traversal instead."""
     layout = layout or infer_layout(tree)
     n = _num_records(tree, layout) if n is None else n
     nq = queries.shape[0]
@@ -622,7 +627,7 @@ def knn_learned(tree, queries, k, model, method="stack_based", layout=None, worl
     fb = torch.zeros(2, dtype=torch.int32, device=dev)
     v = torch.zeros(nq, dtype=torch.int64, device=dev) if visits else None
     st = torch.zeros(nq, dtype=torch.int32, device=dev) if status else None
-    p = _params(method, k, math.inf, 0.0, INT64_MAX, morton)
+    p = _params(method, k, math.inf, 0.0, INT64_MAX, morton, warp_packet=warp_packet)
     _check(lib().cukd_knn_learned(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
                                   _ptr(queries.contiguous()), nq, C.byref(p), model.h, scale,
                                   _ptr(ids), _ptr(d2), _ptr(fb), _ptr(st), _ptr(v),

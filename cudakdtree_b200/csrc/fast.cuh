@@ -24,6 +24,10 @@ struct FastArgs {
 // (register list up to k = 32, local-memory heap above).
 int run_fast(const fast::FastArgs &fa, int D, cudaStream_t st);
 
+// The warp-cooperative traversal (packet.cu): float kNN, k = 2..32, no
+// forest, no device-side query count.
+int run_packet(const fast::FastArgs &fa, int D, cudaStream_t st);
+
 // The same for int32 trees (exact int64 distances), kNN with k = 2..128
 // (fast_int.cu).
 int run_fast_int(const fast::FastArgs &fa, int D, cudaStream_t st);

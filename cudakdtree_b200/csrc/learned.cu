@@ -732,7 +732,8 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   fa.radius_scale = radius_scale;
   fa.status = d_status;
   const bool isFloat = L.scalar == CUKD_FLOAT32;
-  if (isFloat && p->k <= 32) {
+  const bool packet = (p->flags & CUKD_QUERY_WARP_PACKET) && isFloat && p->k <= 32;
+  if (isFloat && p->k <= 32 && !packet) {
     // pass 1: radii predicted and searched in one kernel
     const int D = L.D;
     const int rc = D == 2 ? launch_learned_layout<2>(fa, L, m->d.wbf, m->d.dens, m->norm, st)
@@ -746,7 +747,8 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
     CKB_TRY(arena.alloc(&radius, nq));
     CKB_TRY(infer_launch(m, d_queries, nq, radius, st));
     fa.radius = radius;
-    CKB_TRY(isFloat ? run_fast(fa, L.D, st) : run_fast_int(fa, L.D, st));
+    CKB_TRY(packet ? run_packet(fa, L.D, st)
+                   : (isFloat ? run_fast(fa, L.D, st) : run_fast_int(fa, L.D, st)));
   }
   // pass 2: plain unbounded traversal of the queries pass 1 could not answer
   fast::FastArgs fb = fa;

@@ -274,7 +274,10 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
     fa.work = ctr;
     fa.fb_count = ctr + 1;
     CKB_TRY(arena.alloc(&fa.fb_list, nq));
-    CKB_TRY(L.scalar == CUKD_FLOAT32 ? run_fast(fa, L.D, st) : run_fast_int(fa, L.D, st));
+    const bool packet = (p->flags & CUKD_QUERY_WARP_PACKET) && L.scalar == CUKD_FLOAT32 &&
+                        knn && p->k <= 32;
+    CKB_TRY(packet ? run_packet(fa, L.D, st)
+                   : (L.scalar == CUKD_FLOAT32 ? run_fast(fa, L.D, st) : run_fast_int(fa, L.D, st)));
     if (p->d_reordered_count)
       CKB_CUDA(cudaMemcpyAsync(p->d_reordered_count, fa.fb_count, sizeof(int),
                                cudaMemcpyDeviceToDevice, st));

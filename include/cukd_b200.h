@@ -188,7 +188,13 @@ enum {
    * (left / right bits, root first) instead of by Morton code: an order
    * adapted to the tree's own splits; results are unchanged.  Takes
    * precedence over CUKD_QUERY_MORTON. */
-  CUKD_QUERY_TREE_ORDER = 16
+  CUKD_QUERY_TREE_ORDER = 16,
+  /* float kNN with k = 2..32: the warp-cooperative traversal (the 32
+   * lanes of a warp walk one node stream for 32 consecutive queries of
+   * the visiting order, entering a subtree when any lane's box distance is
+   * within that lane's bound) instead of one traversal per thread; the
+   * same answers (cukd_knn and cukd_knn_learned) */
+  CUKD_QUERY_WARP_PACKET = 32
 };
 
 typedef struct cukd_query_params {

@@ -221,3 +221,42 @@ def test_int_tie_heavy_and_cutoff(mname, m, k, cutoff_d2):
                      world_bounds=torch.from_numpy(bounds).cuda(), cutoff_d2=cutoff_d2)
     assert np.array_equal(ids.cpu().numpy(), ri)
     assert np.array_equal(d2.cpu().numpy(), rd)
+
+
+@pytest.mark.parametrize("D", [2, 3, 4])
+@pytest.mark.parametrize("kind", ["uniform", "tie", "gmm"])
+@pytest.mark.parametrize("k", [2, 8, 16, 32])
+def test_warp_packet_traversal_identical(D, kind, k):
+    """The warp-cooperative traversal (CUKD_QUERY_WARP_PACKET) returns the
+    oracle's ids and distance bits, like the per-thread fast path."""
+    n, nq = 40000, 5003  # a partial last warp
+    pts = make_points(n, D, kind, seed=D + k)
+    q = make_queries(nq, D, kind, seed=D + 2 * k)
+    perm, _, bounds = po.build(pts)
+    t = torch.from_numpy(pts).cuda()
+    wb = ck.build_tree(t)
+    for name, m in (("stack_based", po.STACK_BASED), ("stack_free", po.STACK_FREE)):
+        ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), k, name, world_bounds=wb,
+                         warp_packet=True)
+        ri, rd, _ = po.knn(pts[perm], q, k, m, bounds=bounds)
+        assert np.array_equal(ids.cpu().numpy(), ri)
+        assert np.array_equal(f32_bits(d2.cpu().numpy()), f32_bits(rd))
+    # with a cut-off radius (unfilled slots)
+    ids, d2 = ck.knn(t, torch.from_numpy(q).cuda(), k, world_bounds=wb, cutoff=0.02,
+                     warp_packet=True)
+    pi, pd = ck.knn(t, torch.from_numpy(q).cuda(), k, world_bounds=wb, cutoff=0.02)
+    assert torch.equal(ids, pi) and torch.equal(d2, pd)
+
+
+def test_warp_packet_seeded_by_learned_radius_identical():
+    n = 200000
+    pts = make_points(n, 3, "gmm", seed=1)
+    t = torch.from_numpy(pts).cuda()
+    wb = ck.build_tree(t)
+    m = ck.RadiusModel(seed=2, quantile=0.9)
+    m.fit(t, torch.from_numpy(make_queries(30000, 3, "gmm", seed=3)).cuda(), 16,
+          world_bounds=wb, epochs=4)
+    q = torch.from_numpy(make_queries(40000, 3, "gmm", seed=4)).cuda()
+    pi, pd = ck.knn(t, q, 16, world_bounds=wb)
+    li, ld, fb, _ = ck.knn_learned(t, q, 16, m, world_bounds=wb, warp_packet=True)
+    assert torch.equal(li, pi) and torch.equal(ld, pd)
