@@ -214,6 +214,10 @@ inline bool make_layout(const cukd_layout *l, Layout *out)
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Largest tree the traversals accept: their node indices are 32-bit ints (as
+// the reference's are), and a node's children 2i+1, 2i+2 must fit one.
+constexpr int64_t kMaxQueryTree = (int64_t(1) << 30) - 1;
+
 constexpr int kNumSMs = 148;
 
 }  // namespace ckb

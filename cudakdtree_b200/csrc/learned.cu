@@ -686,7 +686,8 @@ int cukd_knn_learned(const void *d_tree, int64_t n, const cukd_layout *layout,
   ckb::Layout L;
   if (!m || !p || !make_layout(layout, &L) || L.D != m->norm.D || L.scalar != m->scalar)
     return CUKD_ERR_INVALID_ARGUMENT;
-  if (p->k < 2 || p->k > 128 || (p->flags & CUKD_QUERY_HEAP_ORDER) || radius_scale <= 0.f)
+  if (p->k < 2 || p->k > 128 || (p->flags & CUKD_QUERY_HEAP_ORDER) || radius_scale <= 0.f ||
+      n > kMaxQueryTree)
     return CUKD_ERR_UNSUPPORTED;
   if (nq == 0) return CUKD_OK;
   if (!d_queries || !d_out_ids || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;

@@ -197,7 +197,8 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   using namespace query;
   Layout L;
   if (!make_layout(layout, &L) || !p) return CUKD_ERR_INVALID_ARGUMENT;
-  if (nq < 0 || n < 0 || n > (int64_t(1) << 31) - 1) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq < 0 || n < 0) return CUKD_ERR_INVALID_ARGUMENT;
+  if (n > kMaxQueryTree) return CUKD_ERR_UNSUPPORTED;
   if (nq == 0) return CUKD_OK;
   if (!d_queries || (!ids && !visits) || (n > 0 && !d_tree)) return CUKD_ERR_INVALID_ARGUMENT;
   if (p->method < CUKD_STACK_BASED || p->method > CUKD_CCT) return CUKD_ERR_INVALID_ARGUMENT;

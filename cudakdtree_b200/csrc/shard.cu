@@ -234,8 +234,8 @@ int cukd_knn_accumulate(const void *d_tree, int64_t n, const cukd_layout *layout
   Layout L;
   if (!make_layout(layout, &L) || L.scalar != CUKD_FLOAT32) return CUKD_ERR_INVALID_ARGUMENT;
   if (n < 0 || nq < 0 || k < 1 || k > 128) return CUKD_ERR_INVALID_ARGUMENT;
-  if (n > (int64_t(1) << 31) - 1 || id_offset < 0 || id_offset + n > int64_t(0xffffffffll))
-    return CUKD_ERR_INVALID_ARGUMENT;
+  if (id_offset < 0 || id_offset + n > int64_t(0xffffffffll)) return CUKD_ERR_INVALID_ARGUMENT;
+  if (n > kMaxQueryTree) return CUKD_ERR_UNSUPPORTED;
   if (nq == 0) return CUKD_OK;
   if (!d_queries || !d_lists || (n > 0 && !d_tree) || !(max_radius >= 0.f))
     return CUKD_ERR_INVALID_ARGUMENT;

@@ -213,6 +213,11 @@ typedef struct cukd_query_params {
 /* Default parameters: stack-based, k = 8, no cut-off, Morton on. */
 CUKD_API void cukd_query_params_init(cukd_query_params *p);
 
+/* Every query entry point below takes trees of at most 2^30 - 1 nodes and
+ * returns CUKD_ERR_UNSUPPORTED for larger ones: node indices are 32-bit ints
+ * (as in the reference's traversals) and a node's children 2i+1, 2i+2 must
+ * fit one. */
+
 /* Find-closest-point for nq queries (point_t[nq]: num_dims contiguous
  * scalars each).  d_out_ids[i] = node index of the closest point within the
  * cut-off, -1 if none (cukd/fcp.h:54-163, FCPResult :179-207).  For float

@@ -260,3 +260,19 @@ def test_warp_packet_seeded_by_learned_radius_identical():
     pi, pd = ck.knn(t, q, 16, world_bounds=wb)
     li, ld, fb, _ = ck.knn_learned(t, q, 16, m, world_bounds=wb, warp_packet=True)
     assert torch.equal(li, pi) and torch.equal(ld, pd)
+
+
+def test_trees_beyond_32_bit_child_indices_are_refused():
+    """Trees of 2^30 nodes or more would overflow the traversals' 32-bit
+    child indices (2i+1): refused with CUKD_ERR_UNSUPPORTED before any
+    launch (the buffer is never read)."""
+    import ctypes as C
+    t = torch.zeros((16, 3), dtype=torch.float32, device="cuda")
+    q = torch.zeros((4, 3), dtype=torch.float32, device="cuda")
+    ids = torch.empty((4, 8), dtype=torch.int32, device="cuda")
+    d2 = torch.empty((4, 8), dtype=torch.float32, device="cuda")
+    lay = ck.layout_for("float32", 3)
+    p = ck._params("stack_based", 8)
+    rc = ck.lib().cukd_knn(t.data_ptr(), 1 << 30, C.byref(lay), None, q.data_ptr(), 4,
+                           C.byref(p), ids.data_ptr(), d2.data_ptr(), None, None, None)
+    assert rc == 5  # CUKD_ERR_UNSUPPORTED
