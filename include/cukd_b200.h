@@ -53,7 +53,10 @@ typedef enum cukd_status {
    * (cukd/knn.h:620-623 prints "STACK OVERFLOW") */
   CUKD_ERR_STACK_OVERFLOW = 7,
   /* input exceeds the fixed scratch of cukd_build_tree_noalloc */
-  CUKD_ERR_TOO_LARGE = 8
+  CUKD_ERR_TOO_LARGE = 8,
+  /* a consistency check inside a builder failed (reported by
+   * cukd_build_check; the records hold a permutation of the input) */
+  CUKD_ERR_INTERNAL = 9
 } cukd_status;
 
 /* ------------------------------------------------------------------------

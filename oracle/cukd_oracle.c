@@ -267,22 +267,28 @@ static int composite_cmp(const check_ctx *c, int64_t i, int64_t a)
   return c->index[i] < c->index[a] ? -1 : (c->index[a] < c->index[i] ? 1 : 0);
 }
 
-int64_t cko_check_tree(int scalar, int D, const void *tree, const int64_t *index,
-                       const int32_t *dims, int64_t n, const void *bounds, int nthreads)
+static int64_t check_tree_impl(int scalar, int D, const void *tree, const int64_t *index,
+                               const int32_t *dims, int64_t n, const void *bounds, int nthreads)
 {
   if (D < 1 || D > 8 || (dims && !bounds)) return -1;
   check_ctx c = {scalar, D, (const float *)tree, (const int32_t *)tree, index, dims};
   int64_t bad = 0;
 #pragma omp parallel for schedule(dynamic, 4096) reduction(+ : bad) num_threads(nthreads)
   for (int64_t i = 0; i < n; i++) {
-    /* ordering against every ancestor */
+    /* ordering against every ancestor: the canonical composite order, or
+       (no index) only the k-d property, ties on either side */
     int64_t path[64];
     int depth = 0;
     for (int64_t child = i; child > 0;) {
       const int64_t a = (child - 1) / 2;
-      const int r = composite_cmp(&c, i, a);
       const int inLeft = child == 2 * a + 1;
-      if (inLeft ? r >= 0 : r <= 0) bad++;
+      if (index) {
+        const int r = composite_cmp(&c, i, a);
+        if (inLeft ? r >= 0 : r <= 0) bad++;
+      } else {
+        const int r = coord_cmp(&c, i, a, node_dim(&c, a));
+        if (inLeft ? r > 0 : r < 0) bad++;
+      }
       path[depth++] = child;
       child = a;
     }
@@ -312,6 +318,30 @@ int64_t cko_check_tree(int scalar, int D, const void *tree, const int64_t *index
     }
   }
   return bad;
+}
+
+/* Violations of the canonical tree (reference buildTree_host order,
+   builder_host.h): every point is on the correct side of every ancestor in
+   the ancestor's composite order (its split coordinate, then its
+   ancestors' split coordinates, then the input index), and explicit dims
+   are the widest extent of each node's domain box. */
+int64_t cko_check_tree(int scalar, int D, const void *tree, const int64_t *index,
+                       const int32_t *dims, int64_t n, const void *bounds, int nthreads)
+{
+  if (!index) return -1;
+  return check_tree_impl(scalar, D, tree, index, dims, n, bounds, nthreads);
+}
+
+/* Violations of the k-d property alone (any valid left-balanced k-d tree,
+   the guarantee of the reference's builders when points share coordinates,
+   testing/testBuildersSameResult.cu:96-99; checkRec of
+   floatN-knn-and-fcp.cu:387-470): every point of a node's left subtree has
+   split coordinate <= the node's, of its right subtree >=; explicit dims as
+   above. */
+int64_t cko_check_kd(int scalar, int D, const void *tree, const int32_t *dims, int64_t n,
+                     const void *bounds, int nthreads)
+{
+  return check_tree_impl(scalar, D, tree, NULL, dims, n, bounds, nthreads);
 }
 
 /* ===================================================================== */

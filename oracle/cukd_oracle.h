@@ -47,6 +47,9 @@ int cko_build(int scalar, int D, const void *coords, int64_t n, int explicit_dim
  * Returns the number of violations (0 = canonical), -1 on bad arguments. */
 int64_t cko_check_tree(int scalar, int D, const void *tree, const int64_t *index,
                        const int32_t *dims, int64_t n, const void *bounds, int nthreads);
+/* violations of the k-d property alone (ties on either side allowed) */
+int64_t cko_check_kd(int scalar, int D, const void *tree, const int32_t *dims, int64_t n,
+                     const void *bounds, int nthreads);
 
 /* Number of nodes in the subtree under `node` of a left-balanced tree of n
  * nodes. */

@@ -58,6 +58,8 @@ def lib():
         L.cko_build.argtypes = [C.c_int, C.c_int, _P, _I64, C.c_int, _P, _P, _P]
         L.cko_check_tree.argtypes = [C.c_int, C.c_int, _P, _P, _P, _I64, _P, C.c_int]
         L.cko_check_tree.restype = _I64
+        L.cko_check_kd.argtypes = [C.c_int, C.c_int, _P, _P, _I64, _P, C.c_int]
+        L.cko_check_kd.restype = _I64
         L.cko_subtree_size.argtypes = [_I64, _I64]
         L.cko_subtree_size.restype = _I64
         L.cko_fcp.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _I64, _P, _P, _I64, C.c_float,
@@ -157,6 +159,21 @@ def check_tree(tree, index, dims=None, bounds=None, threads=None):
                              threads or nthreads())
     if r < 0:
         raise ValueError("cko_check_tree: bad arguments")
+    return int(r)
+
+
+def check_kd(tree, dims=None, bounds=None, threads=None):
+    """Violations of the k-d property alone (0 = a valid left-balanced k-d
+    tree; points equal to a split coordinate may sit on either side):
+    tree [n, D] coordinates in node order, dims per node for explicit-dim
+    trees (with the world bounds they were built in)."""
+    tree = np.ascontiguousarray(tree)
+    n, D = tree.shape
+    d = None if dims is None else np.ascontiguousarray(dims, np.int32)
+    b = None if bounds is None else np.ascontiguousarray(bounds, dtype=tree.dtype)
+    r = lib().cko_check_kd(_scalar(tree), D, _ptr(tree), _ptr(d), n, _ptr(b), threads or nthreads())
+    if r < 0:
+        raise ValueError("cko_check_kd: bad arguments")
     return int(r)
 
 

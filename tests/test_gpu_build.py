@@ -189,14 +189,12 @@ def test_partition_staging_waits_never_give_up():
     barrier with a bounded poll count; after builds whose chunks start and
     end at every 16-byte phase (sizes 4097..4100 and a 10^6-point build)
     no wait has given up."""
-    import ctypes
+    before = ck.async_wait_timeouts()  # other tests make waits run out on purpose
     for n in (4097, 4098, 4099, 4100, 1_000_000):
         t = torch.from_numpy(make_points(n, 3, "gmm", seed=n)).cuda()
         ck.build_tree(t)
     torch.cuda.synchronize()
-    count = ctypes.c_uint(7)
-    assert ck.lib().cukd_async_wait_timeouts(ctypes.byref(count)) == 0
-    assert count.value == 0
+    assert ck.async_wait_timeouts() == before
 
 
 @pytest.mark.parametrize("offset", [4, 8, 12])

@@ -309,6 +309,37 @@ def test_check_tree_rejects_perturbed_trees(explicit):
         assert po.check_tree(tree, idx, d4, bounds) > 0
 
 
+@pytest.mark.parametrize("explicit", [False, True])
+def test_check_kd_accepts_valid_trees_and_rejects_broken_ones(explicit):
+    """The k-d validity checker: every canonical tree passes, and so does a
+    canonical tree with two equal points exchanged (a different but valid
+    tree, which the canonical checker rejects); exchanging points that
+    differ, or a wrong explicit dim, is caught."""
+    rng = np.random.Generator(np.random.MT19937(11))
+    n = 3001
+    pts = rng.integers(0, 5, size=(n, 3)).astype(np.float32)
+    perm, dims, bounds = po.build(pts, explicit_dim=explicit)
+    dm = dims if explicit else None
+    bd = bounds if explicit else None
+    tree = pts[perm].copy()
+    assert po.check_kd(tree, dm, bd) == 0
+    eq = [(a, b) for a in range(1, n) for b in range(a + 1, min(n, a + 400))
+          if np.array_equal(tree[a], tree[b])][:1]
+    a, b = eq[0]
+    idx = perm.astype(np.int64)
+    x2 = idx.copy()
+    x2[[a, b]] = x2[[b, a]]
+    assert po.check_kd(tree, dm, bd) == 0 and po.check_tree(tree, x2, dm, bd) > 0
+    t3 = tree.copy()
+    t3[[5, 2900]] = t3[[2900, 5]]
+    assert not np.array_equal(tree[5], tree[2900])
+    assert po.check_kd(t3, dm, bd) > 0
+    if explicit:
+        d4 = dims.copy()
+        d4[17] = (d4[17] + 1) % 3
+        assert po.check_kd(tree, d4, bounds) > 0
+
+
 @needs_ref
 @pytest.mark.parametrize("n", [1000, 40000])
 def test_check_tree_accepts_reference_host_builds(n):
