@@ -21,10 +21,12 @@
 //   split    the left set's points above the pivot are paired, k-th with
 //            k-th, with the right set's points below it, and swapped.
 // Levels with at most kMultiSegs subtrees spread every subtree over all
-// CTAs (per-subtree digit histograms in global memory; per-chunk counts of
-// misplaced points, a scan, and pairing in rounds of kPairs through a fixed
-// buffer); deeper levels give each subtree one CTA (histogram in shared
-// memory, misplaced points streamed through two shared-memory rings).  One
+// CTAs: per-subtree digit histograms in global memory; per-chunk counts of
+// misplaced points and a scan of them into ranks; for each left chunk the
+// right-side position of its first rank; then each left chunk pairs its
+// misplaced points with the right side's points of the same ranks.  Deeper
+// levels give each subtree one CTA (histogram in shared memory, misplaced
+// points of both sides streamed through two shared-memory rings).  One
 // cooperative launch runs all of those levels, separated by grid barriers
 // whose waits are bounded.  Subtrees of <= kTile points then finish in
 // shared memory (subtree.cuh), gathered from and written back to their node
@@ -48,8 +50,8 @@
 // -- a property of the record, not of its position -- so the pairing rounds
 // can recount a chunk after earlier rounds swapped part of it.
 //
-// Temporary memory: about 7 MB, independent of n (in place); plus 4 bytes
-// per point (bitonic).
+// Temporary memory: about 5.5 MB, independent of n (in place); plus 4
+// bytes per point (bitonic).
 #include <algorithm>
 #include <mutex>
 
@@ -80,10 +82,9 @@ constexpr int kMultiSegs = 128;
 // record words the in-place tie-break compares after the coordinates
 constexpr int kMaxRaw = 60;
 constexpr int kMaxWords = 4 + kMaxRaw;
-constexpr int kPairs = 1 << 18;      // misplaced pairs per round
 constexpr int kMaxChunks = 1 << 17;  // chunks of a spread level
 constexpr int kMinChunkLog = 12;     // chunks of at least 4096 points
-constexpr int kQueue = 2048;         // ring of misplaced positions, per side
+constexpr int kQueue = 4096;         // ring of misplaced positions, per side
 constexpr int kMaxLevels = 32;
 
 // predicate on a point's comparison with the pivot
@@ -115,21 +116,33 @@ __device__ __forceinline__ void set_dim(const Recs &R, int64_t node, int dim)
   uint32_t *w = (uint32_t *)(R.pts + node * R.stride + R.doff);
   *w = (*w & ~(R.dmask << R.dshift)) | ((uint32_t(dim) & R.dmask) << R.dshift);
 }
+// exchanges two records (and their tags); V16: records are one 16-byte
+// vector each
+template <bool V16>
 __device__ __forceinline__ void swap_recs(const Recs &R, int64_t a, int64_t b)
 {
-  uint32_t *pa = (uint32_t *)(R.pts + a * R.stride);
-  uint32_t *pb = (uint32_t *)(R.pts + b * R.stride);
-  for (int w = 0; w < (R.stride >> 2); w++) {
-    const uint32_t x = pa[w];
-    pa[w] = pb[w];
-    pb[w] = x;
+  if (V16) {
+    uint4 *pa = (uint4 *)(R.pts + a * 16);
+    uint4 *pb = (uint4 *)(R.pts + b * 16);
+    const uint4 x = *pa, y = *pb;
+    *pa = y;
+    *pb = x;
+  } else {
+    uint32_t *pa = (uint32_t *)(R.pts + a * R.stride);
+    uint32_t *pb = (uint32_t *)(R.pts + b * R.stride);
+    for (int w = 0; w < (R.stride >> 2); w++) {
+      const uint32_t x = pa[w], y = pb[w];
+      pa[w] = y;
+      pb[w] = x;
+    }
   }
   if (R.idx) {
-    const uint32_t x = R.idx[a];
-    R.idx[a] = R.idx[b];
+    const uint32_t x = R.idx[a], y = R.idx[b];
+    R.idx[a] = y;
     R.idx[b] = x;
   }
 }
+
 // a consistency check failed: the build stops (status) and
 // cukd_build_check reports CUKD_ERR_INTERNAL; the access is skipped
 __device__ __forceinline__ void build_fault(uint32_t *status)
@@ -151,29 +164,6 @@ __device__ __forceinline__ uint32_t word_of(const Recs &R, int64_t node, int cod
   return off == R.doff ? v & ~(R.dmask << R.dshift) : v;
 }
 
-// domain box of node g (level L) as keys: the world box cut by the split
-// planes of g's ancestors (builder_thrust.h:238-306, builder_common.h
-// findBounds)
-template <int SC, int D>
-__device__ void domain_box(const Recs &R, const uint32_t *wb, bool explicitDims, int L, int64_t g,
-                           uint32_t *lo, uint32_t *hi)
-{
-  for (int d = 0; d < D; d++) {
-    lo[d] = wb[d];
-    hi[d] = wb[D + d];
-  }
-  for (int k = 0; k < L; k++) {
-    const int64_t a = ((g + 1) >> (L - k)) - 1;
-    const int64_t c = ((g + 1) >> (L - k - 1)) - 1;
-    const int da = explicitDims ? dim_at(R, a) : k % D;
-    const uint32_t pc = coord_key<SC>(R, a, da);
-    if (c == 2 * a + 1)
-      hi[da] = pc;
-    else
-      lo[da] = pc;
-  }
-}
-
 // one subtree of the current level
 struct Seg {
   int64_t g, m, r;  // root node, points, rank of the pivot (left subtree size)
@@ -182,12 +172,25 @@ struct Seg {
   int8_t code[kMaxWords];
 };
 
+// Subtree g (level L) from its ancestors' split dims and split coordinates
+// (as keys), ancDim[k] / ancKey[k] for the ancestor on level k.
 template <int SC, int D>
 __device__ void seg_setup(const Recs &R, const uint32_t *wb, bool explicitDims, int L, int64_t g,
-                          Seg &S)
+                          const int8_t *ancDim, const uint32_t *ancKey, Seg &S)
 {
   uint32_t lo[D], hi[D];
-  domain_box<SC, D>(R, wb, explicitDims, L, g, lo, hi);
+  for (int d = 0; d < D; d++) {
+    lo[d] = wb[d];
+    hi[d] = wb[D + d];
+  }
+  for (int k = 0; k < L; k++) {
+    const int64_t a = ((g + 1) >> (L - k)) - 1;
+    const int64_t c = ((g + 1) >> (L - k - 1)) - 1;
+    if (c == 2 * a + 1)
+      hi[ancDim[k]] = ancKey[k];
+    else
+      lo[ancDim[k]] = ancKey[k];
+  }
   S.g = g;
   S.m = subtree_size(g, R.n);
   S.r = left_size(g, R.n);
@@ -198,9 +201,8 @@ __device__ void seg_setup(const Recs &R, const uint32_t *wb, bool explicitDims, 
   int cd[D];
   int ncd = 0;
   cd[ncd++] = S.dim;
-  for (int64_t an = g; an > 0 && ncd < D;) {
-    an = (an - 1) >> 1;
-    const int da = explicitDims ? dim_at(R, an) : level_of(an) % D;
+  for (int k = L - 1; k >= 0 && ncd < D; k--) {
+    const int da = ancDim[k];
     bool seen = false;
     for (int i = 0; i < ncd; i++) seen |= cd[i] == da;
     if (!seen) cd[ncd++] = da;
@@ -254,14 +256,20 @@ __device__ void sel_begin_word(Sel &s, const Seg &S, int64_t n)
   }
 }
 
-// does `node` match the resolved prefix, and its digit of the current word
+// does `node` match the resolved prefix, and its digit of the current word;
+// w0 is the node's first word, already loaded
 template <int SC>
 __device__ __forceinline__ bool sel_digit(const Recs &R, int64_t node, const Seg &S, const Sel &s,
-                                          uint32_t &dg)
+                                          uint32_t w0, uint32_t &dg)
 {
-  for (int x = 0; x < s.w; x++)
-    if (word_of<SC>(R, node, S.code[x]) != s.pw[x]) return false;
-  const uint32_t v = word_of<SC>(R, node, S.code[s.w]) - s.base;
+  uint32_t v = w0;
+  if (s.w > 0) {
+    if (w0 != s.pw[0]) return false;
+    for (int x = 1; x < s.w; x++)
+      if (word_of<SC>(R, node, S.code[x]) != s.pw[x]) return false;
+    v = word_of<SC>(R, node, S.code[s.w]);
+  }
+  v -= s.base;
   if ((v & s.cm) != s.cp) return false;
   dg = (v >> s.shift) & ((1u << s.width) - 1u);
   return true;
@@ -295,11 +303,14 @@ __device__ void sel_advance(Sel &s, const Seg &S, int64_t n, uint32_t dg, uint32
   s.width = wd;
 }
 
+// sign of (record at node) - (pivot) in the composite order; w0 is the
+// node's first word, already loaded
 template <int SC>
 __device__ __forceinline__ int cmp_pivot(const Recs &R, int64_t node, const Seg &S,
-                                         const uint32_t *pk)
+                                         const uint32_t *pk, uint32_t w0)
 {
-  for (int x = 0; x < S.nwords; x++) {
+  if (w0 != pk[0]) return w0 < pk[0] ? -1 : 1;
+  for (int x = 1; x < S.nwords; x++) {
     const uint32_t v = word_of<SC>(R, node, S.code[x]);
     if (v != pk[x]) return v < pk[x] ? -1 : 1;
   }
@@ -340,6 +351,43 @@ __device__ __forceinline__ void chunk_pos(int64_t t, int lc, int &j, int64_t &k)
   j = lc + 1 + i;
   k = tp - (int64_t(1) << i);
 }
+// chunk t of side sd of subtree g: first node and length
+__device__ __forceinline__ void chunk_range(int64_t g, int sd, int64_t t, int lc, int64_t n,
+                                            int64_t &cs, int64_t &cl)
+{
+  int j;
+  int64_t k;
+  chunk_pos(t, lc, j, k);
+  int64_t hs, hl;
+  half_run(g, j, sd, n, hs, hl);
+  const int64_t C = int64_t(1) << lc;
+  cs = hs + (k << lc);
+  cl = hl - (k << lc);
+  cl = cl < 0 ? 0 : (cl > C ? C : cl);
+}
+
+// the v-th node of subtree g's node set, depth by depth
+__device__ __forceinline__ int64_t set_node(int64_t g, int64_t v)
+{
+  const int j = 63 - __clzll((long long)(v + 1));
+  return ((g + 1) << j) - 1 + (v - ((int64_t(1) << j) - 1));
+}
+// the v-th node of side sd (0 left, 1 right) of subtree g, depth by depth
+__device__ __forceinline__ int64_t side_node(int64_t g, int sd, int64_t v)
+{
+  const int jj = 63 - __clzll((long long)(v + 1));  // depth - 1
+  const int64_t half = int64_t(1) << jj;
+  return ((g + 1) << (jj + 1)) - 1 + sd * half + (v - (half - 1));
+}
+
+// points per thread per batch in the streaming loops (independent loads in
+// flight per thread)
+constexpr int kU = 4;
+constexpr int kBatch = kThreads * kU;
+// the histogram and count passes over chunks: 16 per thread, a whole
+// 4096-point chunk per batch
+constexpr int kUs = 8;
+constexpr int kBatchS = kThreads * kUs;
 
 struct TopArgs {
   Recs R;
@@ -353,9 +401,8 @@ struct TopArgs {
   Sel *sel;
   uint32_t *hist, *hpos;  // [kMultiSegs][kBins]
   uint32_t *ccnt, *cst;   // [kMaxChunks]
+  uint32_t *bnd;          // [kMaxChunks][2]: partner chunk and offset of a left chunk
   uint32_t *tot;          // [2 phases][2 * kMultiSegs]
-  uint32_t *pairs;        // [2][npairs]
-  int64_t npairs;         // pairs per round
   int8_t lc[kMaxLevels];  // log2 chunk size per spread level
 };
 
@@ -372,14 +419,16 @@ struct TopSmem {
   uint32_t pk[kMaxWords];
   uint32_t wsum[kThreads / 32];
   uint32_t res[3];
-  int64_t segOff;
-  int64_t segK;
   int cached;
   int ok;
   int pred[2];
-  int qHead[2], qCnt[2], qExh[2], qJ[2];
-  int64_t qOff[2];
-  int err;
+  // rings of misplaced positions, per side: a cursor over a sequence of
+  // node ranges (the side's half-runs by depth, or its chunks)
+  int qHead[2], qCnt[2], qExh[2];
+  int64_t qIdx[2], qEnd[2], qOff[2];
+  int qChunked, qLc;
+  int8_t ancDim[kMaxLevels];
+  uint32_t ancKey[kMaxLevels];
 };
 
 // Grid-wide barrier of the cooperative launch.  The wait is bounded
@@ -405,7 +454,7 @@ __device__ bool grid_barrier(const TopArgs &A, TopSmem &T)
           ok = 0;
           break;
         }
-        __nanosleep(128);
+        __nanosleep(64);
       }
     }
     __threadfence();
@@ -471,6 +520,118 @@ __device__ void find_digit(const uint32_t *h, uint32_t rank, TopSmem &T)
   __syncthreads();
 }
 
+// histogram of the current digit over the nodes [cs, cs + cl) (every
+// thread); true if this thread counted a point
+template <int SC>
+__device__ bool hist_range(const Recs &R, const Seg &S, const Sel &s, int64_t cs, int64_t cl,
+                           uint32_t *hist, uint32_t *hpos)
+{
+  const int code0 = S.code[0];
+  bool any = false;
+  for (int64_t b = 0; b < cl; b += kBatchS) {
+    uint32_t w[kUs];
+#pragma unroll
+    for (int u = 0; u < kUs; u++) {
+      const int64_t e = b + u * kThreads + threadIdx.x;
+      w[u] = e < cl ? word_of<SC>(R, cs + e, code0) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kUs; u++) {
+      const int64_t e = b + u * kThreads + threadIdx.x;
+      uint32_t dg;
+      if (e < cl && sel_digit<SC>(R, cs + e, S, s, w[u], dg)) {
+        atomicAdd(&hist[dg], 1u);
+        hpos[dg] = uint32_t(cs + e);
+        any = true;
+      }
+    }
+  }
+  return any;
+}
+
+// the same over subtree S.g's whole node set, as one flat sequence
+template <int SC>
+__device__ void hist_set(const Recs &R, const Seg &S, const Sel &s, uint32_t *hist, uint32_t *hpos)
+{
+  const int64_t vEnd = (int64_t(2) << S.jmax) - 1;
+  const int code0 = S.code[0];
+  for (int64_t b = 0; b < vEnd; b += kBatch) {
+    int64_t node[kU];
+    uint32_t w[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const int64_t v = b + u * kThreads + threadIdx.x;
+      node[u] = v < vEnd ? set_node(S.g, v) : R.n;
+      w[u] = node[u] < R.n ? word_of<SC>(R, node[u], code0) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      uint32_t dg;
+      if (node[u] < R.n && sel_digit<SC>(R, node[u], S, s, w[u], dg)) {
+        atomicAdd(&hist[dg], 1u);
+        hpos[dg] = uint32_t(node[u]);
+      }
+    }
+  }
+}
+
+// points of [cs, cs + cl) that satisfy pred (this thread's share)
+template <int SC>
+__device__ uint32_t count_range(const Recs &R, const Seg &S, const uint32_t *pk, int pred,
+                                int64_t cs, int64_t cl)
+{
+  const int code0 = S.code[0];
+  uint32_t cnt = 0;
+  for (int64_t b = 0; b < cl; b += kBatchS) {
+    uint32_t w[kUs];
+#pragma unroll
+    for (int u = 0; u < kUs; u++) {
+      const int64_t e = b + u * kThreads + threadIdx.x;
+      w[u] = e < cl ? word_of<SC>(R, cs + e, code0) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kUs; u++) {
+      const int64_t e = b + u * kThreads + threadIdx.x;
+      cnt += (e < cl && pred_hit(cmp_pivot<SC>(R, cs + e, S, pk, w[u]), pred)) ? 1u : 0u;
+    }
+  }
+  return cnt;
+}
+
+// which of this thread's kU consecutive points of the batch at offset b of
+// [cs, cs + cl) satisfy pred (bit u: point b + threadIdx.x * kU + u)
+template <int SC>
+__device__ __forceinline__ uint32_t hit_mask(const Recs &R, const Seg &S, const uint32_t *pk,
+                                             int pred, int64_t cs, int64_t cl, int64_t b)
+{
+  const int64_t e0 = b + int64_t(threadIdx.x) * kU;
+  const int code0 = S.code[0];
+  uint32_t w[kU];
+#pragma unroll
+  for (int u = 0; u < kU; u++) w[u] = e0 + u < cl ? word_of<SC>(R, cs + e0 + u, code0) : 0u;
+  uint32_t m = 0;
+#pragma unroll
+  for (int u = 0; u < kU; u++)
+    if (e0 + u < cl && pred_hit(cmp_pivot<SC>(R, cs + e0 + u, S, pk, w[u]), pred)) m |= 1u << u;
+  return m;
+}
+
+// split dim and split coordinate (key) of every ancestor of g (level L),
+// one thread per ancestor (every thread calls it)
+template <int SC, int D>
+__device__ void load_ancestors(const Recs &R, bool explicitDims, int L, int64_t g, int8_t *ancDim,
+                               uint32_t *ancKey)
+{
+  __syncthreads();
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    const int64_t a = ((g + 1) >> (L - k)) - 1;
+    const int da = explicitDims ? dim_at(R, a) : k % D;
+    ancDim[k] = int8_t(da);
+    ancKey[k] = coord_key<SC>(R, a, da);
+  }
+  __syncthreads();
+}
+
 template <int SC>
 __device__ void place_pivot(const TopArgs &A, const Seg &S, const Sel &s)
 {
@@ -478,7 +639,7 @@ __device__ void place_pivot(const TopArgs &A, const Seg &S, const Sel &s)
     build_fault(A.status);
     return;
   }
-  if (s.pos != S.g) swap_recs(A.R, s.pos, S.g);
+  if (s.pos != S.g) swap_recs<false>(A.R, s.pos, S.g);
   if (A.explicitDims) set_dim(A.R, S.g, S.dim);
 }
 
@@ -503,9 +664,124 @@ __device__ void load_seg(const TopArgs &A, int s, bool withSel, TopSmem &T)
 }
 
 // ---------------------------------------------------------------------------
+// rings of misplaced positions
+// ---------------------------------------------------------------------------
+// node range idx of side sd's cursor: a half-run by depth (one CTA per
+// subtree) or a chunk (spread levels)
+__device__ __forceinline__ void cursor_range(const TopSmem &T, int sd, int64_t idx, int64_t n,
+                                             int64_t &cs, int64_t &cl)
+{
+  if (T.qChunked)
+    chunk_range(T.seg.g, sd, idx, T.qLc, n, cs, cl);
+  else
+    half_run(T.seg.g, int(idx), sd, n, cs, cl);
+}
+
+__device__ void ring_start(int sd, int pred, int64_t idx, int64_t end, int64_t off, TopSmem &T)
+{
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T.qHead[sd] = 0;
+    T.qCnt[sd] = 0;
+    T.qExh[sd] = 0;
+    T.qIdx[sd] = idx;
+    T.qEnd[sd] = end;
+    T.qOff[sd] = off;
+    T.pred[sd] = pred;
+  }
+  __syncthreads();
+}
+
+// appends the side's next misplaced positions, in node order, until the
+// ring holds `want`, is nearly full, or the side is exhausted (all
+// threads; uniform).  Chunked cursors walk chunk ids (qIdx) and an offset
+// in the chunk; flat cursors walk the side's node set by index (qOff, up to
+// qEnd).
+template <int SC>
+__device__ void ring_fill(const Recs &R, int sd, int64_t want, TopSmem &T)
+{
+  const int tid = threadIdx.x;
+  for (;;) {
+    __syncthreads();
+    if (T.qExh[sd] || T.qCnt[sd] >= want || T.qCnt[sd] > kQueue - kBatch) break;
+    const int64_t idx = T.qIdx[sd], off = T.qOff[sd];
+    int64_t cs = 0, cl = T.qEnd[sd];
+    bool next = false, exhausted = false;
+    if (T.qChunked) {
+      if (idx >= T.qEnd[sd])
+        exhausted = true;
+      else {
+        chunk_range(T.seg.g, sd, idx, T.qLc, R.n, cs, cl);
+        next = off >= cl;
+      }
+    } else {
+      exhausted = off >= cl;
+    }
+    if (exhausted || next) {
+      __syncthreads();
+      if (tid == 0) {
+        if (exhausted)
+          T.qExh[sd] = 1;
+        else {
+          T.qIdx[sd] = idx + 1;
+          T.qOff[sd] = 0;
+        }
+      }
+      continue;
+    }
+    const int64_t e0 = off + int64_t(tid) * kU;
+    const int code0 = T.seg.code[0];
+    int64_t node[kU];
+    uint32_t w[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const int64_t e = e0 + u;
+      node[u] = e < cl ? (T.qChunked ? cs + e : side_node(T.seg.g, sd, e)) : R.n;
+      w[u] = node[u] < R.n ? word_of<SC>(R, node[u], code0) : 0u;
+    }
+    uint32_t m = 0;
+#pragma unroll
+    for (int u = 0; u < kU; u++)
+      if (node[u] < R.n && pred_hit(cmp_pivot<SC>(R, node[u], T.seg, T.pk, w[u]), T.pred[sd]))
+        m |= 1u << u;
+    uint32_t total;
+    uint32_t r = block_scan(__popc(m), T, &total);
+    const int tail = T.qHead[sd] + T.qCnt[sd];
+#pragma unroll
+    for (int u = 0; u < kU; u++)
+      if ((m >> u) & 1u) T.u.q[sd][(tail + int(r++)) % kQueue] = uint32_t(node[u]);
+    __syncthreads();
+    if (tid == 0) {
+      T.qCnt[sd] += int(total);
+      T.qOff[sd] = off + (cl - off < kBatch ? cl - off : kBatch);
+    }
+  }
+}
+
+// swaps the rings' first min(count0, count1, limit) pairs; returns it
+template <bool V16>
+__device__ int ring_pair(const Recs &R, int64_t limit, TopSmem &T)
+{
+  __syncthreads();
+  int k = min(T.qCnt[0], T.qCnt[1]);
+  if (int64_t(k) > limit) k = int(limit);
+  for (int i = threadIdx.x; i < k; i += kThreads)
+    swap_recs<V16>(R, T.u.q[0][(T.qHead[0] + i) % kQueue], T.u.q[1][(T.qHead[1] + i) % kQueue]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int sd = 0; sd < 2; sd++) {
+      T.qHead[sd] = (T.qHead[sd] + k) % kQueue;
+      T.qCnt[sd] -= k;
+    }
+  }
+  __syncthreads();
+  return k;
+}
+
+// ---------------------------------------------------------------------------
 // spread level: every subtree over all CTAs
 // ---------------------------------------------------------------------------
-template <int SC, int D>
+template <int SC, int D, bool V16>
 __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
 {
   const Recs &R = A.R;
@@ -518,9 +794,10 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
   const int tid = threadIdx.x;
 
   for (int s = blockIdx.x; s < nseg; s += gridDim.x) {
+    load_ancestors<SC, D>(R, A.explicitDims, L, g0 + s, T.ancDim, T.ancKey);
     if (tid == 0) {
       Seg S;
-      seg_setup<SC, D>(R, A.wb, A.explicitDims, L, g0 + s, S);
+      seg_setup<SC, D>(R, A.wb, A.explicitDims, L, g0 + s, T.ancDim, T.ancKey, S);
       A.seg[s] = S;
       Sel sl;
       sl.w = 0;
@@ -546,6 +823,7 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
     // ended pass p - 1's histograms
     if (blockIdx.x == 0 && tid == 0) A.active[p & 1] = 0;
     if (tid == 0) T.cached = -1;
+    for (int i = tid; i < kBins; i += kThreads) T.u.h.hist[i] = 0;
     __syncthreads();
     for (int64_t id = blockIdx.x; id < nch; id += gridDim.x) {
       const int s = int(id / (2 * cps));
@@ -558,34 +836,26 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
         __syncthreads();
       }
       if (T.sel.done) continue;
-      int j;
-      int64_t k;
-      chunk_pos(t, lc, j, k);
-      int64_t hs, hl;
-      half_run(T.seg.g, j, sd, R.n, hs, hl);
-      const int64_t cs = hs + (k << lc);
-      int64_t cl = hl - (k << lc);
-      cl = cl < 0 ? 0 : (cl > (int64_t(1) << lc) ? (int64_t(1) << lc) : cl);
-      for (int i = tid; i < kBins; i += kThreads) T.u.h.hist[i] = 0;
-      __syncthreads();
+      int64_t cs, cl;
+      chunk_range(T.seg.g, sd, t, lc, R.n, cs, cl);
+      bool any = hist_range<SC>(R, T.seg, T.sel, cs, cl, T.u.h.hist, T.u.h.hpos);
       uint32_t dg;
-      for (int64_t e = tid; e < cl; e += kThreads) {
-        const int64_t node = cs + e;
-        if (sel_digit<SC>(R, node, T.seg, T.sel, dg)) {
-          atomicAdd(&T.u.h.hist[dg], 1u);
-          T.u.h.hpos[dg] = uint32_t(node);
-        }
-      }
-      if (sd == 0 && t == 0 && tid == 0 && sel_digit<SC>(R, T.seg.g, T.seg, T.sel, dg)) {
+      if (sd == 0 && t == 0 && tid == 0 &&
+          sel_digit<SC>(R, T.seg.g, T.seg, T.sel, word_of<SC>(R, T.seg.g, T.seg.code[0]), dg)) {
         atomicAdd(&T.u.h.hist[dg], 1u);
         T.u.h.hpos[dg] = uint32_t(T.seg.g);
+        any = true;
       }
-      __syncthreads();
-      for (int i = tid; i < kBins; i += kThreads) {
-        const uint32_t c = T.u.h.hist[i];
-        if (c) {
-          atomicAdd(&A.hist[int64_t(s) * kBins + i], c);
-          A.hpos[int64_t(s) * kBins + i] = T.u.h.hpos[i];
+      // merge into the subtree's row only if the chunk counted anything
+      // (the bins are zeroed again as they are merged)
+      if (__syncthreads_or(any)) {
+        for (int i = tid; i < kBins; i += kThreads) {
+          const uint32_t c = T.u.h.hist[i];
+          if (c) {
+            atomicAdd(&A.hist[int64_t(s) * kBins + i], c);
+            A.hpos[int64_t(s) * kBins + i] = T.u.h.hpos[i];
+            T.u.h.hist[i] = 0;
+          }
         }
       }
       __syncthreads();
@@ -620,7 +890,12 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
 
   // ---- split: phase 0 pairs points above the pivot in the left set with
   // points below it in the right set; phase 1 (only where the pivot has
-  // byte-identical twins) pairs what is left over with twins
+  // byte-identical twins) pairs what is left over with twins.  Per phase:
+  // count each chunk's misplaced points, scan the counts per (subtree,
+  // side) into ranks, find for every left chunk the right-side position of
+  // its first rank, then let each left chunk swap its misplaced points with
+  // the right side's points of the same ranks (disjoint positions per left
+  // chunk, so no further barrier).
   bool anyUneven = false;
   for (int phase = 0; phase < 2; phase++) {
     if (phase == 1 && !anyUneven) break;
@@ -656,16 +931,9 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
       const int pred = T.pred[sd];
       uint32_t cnt = 0;
       if (pred != kNone) {
-        int j;
-        int64_t k;
-        chunk_pos(t, lc, j, k);
-        int64_t hs, hl;
-        half_run(T.seg.g, j, sd, R.n, hs, hl);
-        const int64_t cs = hs + (k << lc);
-        int64_t cl = hl - (k << lc);
-        cl = cl < 0 ? 0 : (cl > (int64_t(1) << lc) ? (int64_t(1) << lc) : cl);
-        for (int64_t e = tid; e < cl; e += kThreads)
-          cnt += pred_hit(cmp_pivot<SC>(R, cs + e, T.seg, T.pk), pred) ? 1u : 0u;
+        int64_t cs, cl;
+        chunk_range(T.seg.g, sd, t, lc, R.n, cs, cl);
+        cnt = count_range<SC>(R, T.seg, T.pk, pred, cs, cl);
       }
       uint32_t total;
       block_scan(cnt, T, &total);
@@ -686,71 +954,92 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
       if (tid == 0) tot[q] = carry;
     }
     if (!grid_barrier(A, T)) return false;
-    int64_t K = 0;
-    for (int s = 0; s < nseg; s++) {
-      const uint32_t a = tot[2 * s], b = tot[2 * s + 1];
-      K += a < b ? a : b;
-      if (phase == 0 && a != b) anyUneven = true;
-    }
-    for (int64_t r0 = 0; r0 < K; r0 += A.npairs) {
-      if (tid == 0) T.cached = -1;
+    for (int s = 0; s < nseg; s++)
+      if (phase == 0 && tot[2 * s] != tot[2 * s + 1]) anyUneven = true;
+    // partner position of each left chunk's first rank
+    for (int64_t t = blockIdx.x; t < int64_t(nseg) * cps; t += gridDim.x) {
+      const int s = int(t / cps);
+      const int64_t id = int64_t(2 * s) * cps + t % cps;  // the left chunk
+      const uint32_t K = min(tot[2 * s], tot[2 * s + 1]);
+      const uint32_t st = A.cst[id], c = A.ccnt[id];
+      if (c == 0 || st >= K) {
+        if (tid == 0) A.bnd[2 * id] = 0xffffffffu;
+        continue;
+      }
+      cache_seg(s);
+      // the right chunk holding rank st: the last whose first rank is <= st
+      const int64_t rb = int64_t(2 * s + 1) * cps;
+      const int64_t stride = (cps + kThreads - 1) / kThreads;
+      const int64_t probe = int64_t(tid) * stride;
+      const int n1 = __syncthreads_count(probe < cps && A.cst[rb + probe] <= st);
+      const int64_t lo = int64_t(n1 - 1) * stride;
+      const int64_t p2 = lo + tid;
+      const int n2 = __syncthreads_count(tid < stride && p2 < cps && A.cst[rb + p2] <= st);
+      const int64_t jr = lo + n2 - 1;
+      // offset of that rank's point inside the right chunk
+      int64_t cs, cl;
+      chunk_range(T.seg.g, 1, jr % cps, lc, R.n, cs, cl);
+      uint32_t want = st - A.cst[rb + jr];
+      if (tid == 0) T.res[0] = 0xffffffffu;
       __syncthreads();
-      for (int64_t id = blockIdx.x; id < nch; id += gridDim.x) {
-        const int s = int(id / (2 * cps));
-        const int sd = int((id / cps) & 1);
-        const int64_t t = id % cps;
-        if (T.cached != s) {
-          cache_seg(s);
-          if (tid == 0) {
-            int64_t off = 0;
-            for (int x = 0; x < s; x++) off += min(tot[2 * x], tot[2 * x + 1]);
-            T.segOff = off;
-            T.segK = min(tot[2 * s], tot[2 * s + 1]);
-          }
-          __syncthreads();
+      for (int64_t b = 0; b < cl; b += kBatch) {
+        const uint32_t m = hit_mask<SC>(R, T.seg, T.pk, T.pred[1], cs, cl, b);
+        uint32_t total;
+        const uint32_t ex = block_scan(__popc(m), T, &total);
+        if (want >= ex && want < ex + __popc(m)) {
+          uint32_t r = ex;
+#pragma unroll
+          for (int u = 0; u < kU; u++)
+            if ((m >> u) & 1u) {
+              if (r == want) T.res[0] = uint32_t(b + int64_t(tid) * kU + u);
+              r++;
+            }
         }
-        const int pred = T.pred[sd];
-        if (pred == kNone) continue;
-        const int64_t st = A.cst[id], c = A.ccnt[id];
-        const int64_t lo = max(st, r0 - T.segOff);
-        const int64_t hi = min(min(st + c, T.segK), r0 + A.npairs - T.segOff);
-        if (lo >= hi) continue;
-        int j;
-        int64_t k;
-        chunk_pos(t, lc, j, k);
-        int64_t hs, hl;
-        half_run(T.seg.g, j, sd, R.n, hs, hl);
-        const int64_t cs = hs + (k << lc);
-        int64_t cl = hl - (k << lc);
-        cl = cl < 0 ? 0 : (cl > (int64_t(1) << lc) ? (int64_t(1) << lc) : cl);
-        int64_t rank = lo;  // rank of the next misplaced point (uniform)
-        uint32_t *out = A.pairs + sd * A.npairs;
-        for (int64_t b0 = 0; b0 < cl && rank < hi; b0 += kThreads) {
-          const int64_t e = b0 + tid;
-          const bool hit = e < cl && pred_hit(cmp_pivot<SC>(R, cs + e, T.seg, T.pk), pred);
-          uint32_t total;
-          const uint32_t ex = block_scan(hit ? 1u : 0u, T, &total);
-          const int64_t rk = rank + ex;
-          if (hit && rk < hi) out[T.segOff + rk - r0] = uint32_t(cs + e);
-          rank += total;
-        }
+        __syncthreads();
+        if (T.res[0] != 0xffffffffu) break;
+        want -= total;
       }
-      if (!grid_barrier(A, T)) return false;
-      const int64_t np = min(A.npairs, K - r0);
-      // every entry is written by the compaction above; an entry left at
-      // the marker means the counts disagreed
-      for (int64_t i = int64_t(blockIdx.x) * kThreads + tid; i < np;
-           i += int64_t(gridDim.x) * kThreads) {
-        const uint32_t a = A.pairs[i], b = A.pairs[A.npairs + i];
-        A.pairs[i] = 0xffffffffu;
-        A.pairs[A.npairs + i] = 0xffffffffu;
-        if (a >= uint64_t(R.n) || b >= uint64_t(R.n))
-          build_fault(A.status);
-        else
-          swap_recs(R, a, b);
+      if (tid == 0) {
+        A.bnd[2 * id] = uint32_t(jr);
+        A.bnd[2 * id + 1] = T.res[0];
+        if (T.res[0] == 0xffffffffu) A.bnd[2 * id] = 0xfffffffeu;
       }
-      if (!grid_barrier(A, T)) return false;
+      __syncthreads();
     }
+    if (!grid_barrier(A, T)) return false;
+    // pair and swap, one left chunk at a time
+    for (int64_t t = blockIdx.x; t < int64_t(nseg) * cps; t += gridDim.x) {
+      const int s = int(t / cps);
+      const int64_t id = int64_t(2 * s) * cps + t % cps;
+      const uint32_t jr = A.bnd[2 * id];
+      if (jr == 0xffffffffu) continue;
+      cache_seg(s);
+      if (jr == 0xfffffffeu) {  // the counts disagreed
+        if (tid == 0) build_fault(A.status);
+        continue;
+      }
+      const uint32_t K = min(tot[2 * s], tot[2 * s + 1]);
+      const int64_t need = min(int64_t(A.ccnt[id]), int64_t(K) - A.cst[id]);
+      __syncthreads();
+      if (tid == 0) {
+        T.qChunked = 1;
+        T.qLc = lc;
+      }
+      ring_start(0, T.pred[0], t % cps, t % cps + 1, 0, T);
+      ring_start(1, T.pred[1], jr, cps, A.bnd[2 * id + 1], T);
+      int64_t done = 0;
+      while (done < need) {
+        ring_fill<SC>(R, 0, need - done, T);
+        ring_fill<SC>(R, 1, need - done, T);
+        const int k = ring_pair<V16>(R, need - done, T);
+        if (k == 0) {
+          if (tid == 0) build_fault(A.status);
+          break;
+        }
+        done += k;
+      }
+    }
+    if (!grid_barrier(A, T)) return false;
   }
   return true;
 }
@@ -758,85 +1047,21 @@ __device__ bool spread_level(const TopArgs &A, int L, TopSmem &T)
 // ---------------------------------------------------------------------------
 // CTA-per-subtree level
 // ---------------------------------------------------------------------------
-// appends the side's next misplaced positions to its ring until it is
-// nearly full or the side is exhausted (all threads; uniform)
-template <int SC>
-__device__ void ring_fill(const Recs &R, int sd, TopSmem &T)
-{
-  const int tid = threadIdx.x;
-  for (;;) {
-    __syncthreads();
-    if (T.qExh[sd] || T.qCnt[sd] > kQueue - kThreads) break;
-    const int j = T.qJ[sd];
-    if (j > T.seg.jmax) {
-      __syncthreads();
-      if (tid == 0) T.qExh[sd] = 1;
-      continue;
-    }
-    int64_t hs, hl;
-    half_run(T.seg.g, j, sd, R.n, hs, hl);
-    const int64_t off = T.qOff[sd];
-    if (off >= hl) {
-      __syncthreads();
-      if (tid == 0) {
-        T.qJ[sd] = j + 1;
-        T.qOff[sd] = 0;
-      }
-      continue;
-    }
-    const int64_t e = off + tid;
-    const bool hit = e < hl && pred_hit(cmp_pivot<SC>(R, hs + e, T.seg, T.pk), T.pred[sd]);
-    uint32_t total;
-    const uint32_t ex = block_scan(hit ? 1u : 0u, T, &total);
-    if (hit) T.u.q[sd][(T.qHead[sd] + T.qCnt[sd] + int(ex)) % kQueue] = uint32_t(hs + e);
-    __syncthreads();
-    if (tid == 0) {
-      T.qCnt[sd] += int(total);
-      const int64_t step = hl - off < kThreads ? hl - off : kThreads;
-      T.qOff[sd] = off + step;
-    }
-  }
-}
-
-template <int SC>
-__device__ void ring_restart(int sd, int pred, TopSmem &T)
-{
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    T.qHead[sd] = 0;
-    T.qCnt[sd] = 0;
-    T.qExh[sd] = 0;
-    T.qJ[sd] = 1;
-    T.qOff[sd] = 0;
-    T.pred[sd] = pred;
-  }
-  __syncthreads();
-}
-
-template <int SC>
+template <int SC, bool V16>
 __device__ void cta_split(const TopArgs &A, TopSmem &T)
 {
   const Recs &R = A.R;
-  ring_restart<SC>(0, kAbove, T);
-  ring_restart<SC>(1, kBelow, T);
+  const int64_t unlimited = int64_t(1) << 62;
+  __syncthreads();
+  if (threadIdx.x == 0) T.qChunked = 0;
+  const int64_t sideEnd = (int64_t(1) << T.seg.jmax) - 1;  // node slots of one side
+  ring_start(0, kAbove, 0, sideEnd, 0, T);
+  ring_start(1, kBelow, 0, sideEnd, 0, T);
   int twinSide = -1;  // side re-scanned for twins of the pivot, once the other is left over
   for (;;) {
-    ring_fill<SC>(R, 0, T);
-    ring_fill<SC>(R, 1, T);
-    __syncthreads();
-    const int k = min(T.qCnt[0], T.qCnt[1]);
-    if (k > 0) {
-      for (int i = threadIdx.x; i < k; i += kThreads)
-        swap_recs(R, T.u.q[0][(T.qHead[0] + i) % kQueue], T.u.q[1][(T.qHead[1] + i) % kQueue]);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        for (int sd = 0; sd < 2; sd++) {
-          T.qHead[sd] = (T.qHead[sd] + k) % kQueue;
-          T.qCnt[sd] -= k;
-        }
-      }
-      continue;
-    }
+    ring_fill<SC>(R, 0, unlimited, T);
+    ring_fill<SC>(R, 1, unlimited, T);
+    if (ring_pair<V16>(R, unlimited, T) > 0) continue;
     const bool done0 = T.qExh[0] && T.qCnt[0] == 0;
     const bool done1 = T.qExh[1] && T.qCnt[1] == 0;
     if (twinSide < 0) {
@@ -844,7 +1069,7 @@ __device__ void cta_split(const TopArgs &A, TopSmem &T)
       // one side has run out: the other's remaining points pair with twins
       // of the pivot from the side that ran out
       twinSide = done1 ? 1 : 0;
-      ring_restart<SC>(twinSide, kTwin, T);
+      ring_start(twinSide, kTwin, 0, sideEnd, 0, T);
       continue;
     }
     // the side paired with twins is finished (twins may be left over)
@@ -857,7 +1082,7 @@ __device__ void cta_split(const TopArgs &A, TopSmem &T)
   __syncthreads();
 }
 
-template <int SC, int D>
+template <int SC, int D, bool V16>
 __device__ bool cta_level(const TopArgs &A, int L, TopSmem &T)
 {
   const Recs &R = A.R;
@@ -865,9 +1090,9 @@ __device__ bool cta_level(const TopArgs &A, int L, TopSmem &T)
   const int64_t g0 = (int64_t(1) << L) - 1;
   const int tid = threadIdx.x;
   for (int s = blockIdx.x; s < nseg; s += gridDim.x) {
-    __syncthreads();
+    load_ancestors<SC, D>(R, A.explicitDims, L, g0 + s, T.ancDim, T.ancKey);
     if (tid == 0) {
-      seg_setup<SC, D>(R, A.wb, A.explicitDims, L, g0 + s, T.seg);
+      seg_setup<SC, D>(R, A.wb, A.explicitDims, L, g0 + s, T.ancDim, T.ancKey, T.seg);
       Sel &sl = T.sel;
       sl.w = 0;
       sl.done = 0;
@@ -884,18 +1109,7 @@ __device__ bool cta_level(const TopArgs &A, int L, TopSmem &T)
     while (!T.sel.done) {
       for (int i = tid; i < kBins; i += kThreads) T.u.h.hist[i] = 0;
       __syncthreads();
-      uint32_t dg;
-      for (int j = 0; j <= T.seg.jmax; j++) {
-        const int64_t rs = ((T.seg.g + 1) << j) - 1;
-        int64_t rl = R.n - rs;
-        rl = rl < 0 ? 0 : (rl > (int64_t(1) << j) ? (int64_t(1) << j) : rl);
-        for (int64_t e = tid; e < rl; e += kThreads) {
-          if (sel_digit<SC>(R, rs + e, T.seg, T.sel, dg)) {
-            atomicAdd(&T.u.h.hist[dg], 1u);
-            T.u.h.hpos[dg] = uint32_t(rs + e);
-          }
-        }
-      }
+      hist_set<SC>(R, T.seg, T.sel, T.u.h.hist, T.u.h.hpos);
       __syncthreads();
       find_digit(T.u.h.hist, T.sel.rank, T);
       if (tid == 0) {
@@ -907,17 +1121,19 @@ __device__ bool cta_level(const TopArgs &A, int L, TopSmem &T)
     if (tid == 0) place_pivot<SC>(A, T.seg, T.sel);
     __syncthreads();
     load_pivot_words<SC>(A, T);
-    cta_split<SC>(A, T);
+    cta_split<SC, V16>(A, T);
   }
   return grid_barrier(A, T);
 }
 
-template <int SC, int D>
+// V16: 16-byte records at a 16-byte aligned base (swapped as one vector)
+template <int SC, int D, bool V16>
 __global__ void __launch_bounds__(kThreads, 4) top_kernel(TopArgs A)
 {
   __shared__ TopSmem T;
   for (int L = 0; L < A.G; L++) {
-    const bool ok = (1 << L) <= kMultiSegs ? spread_level<SC, D>(A, L, T) : cta_level<SC, D>(A, L, T);
+    const bool ok = (1 << L) <= kMultiSegs ? spread_level<SC, D, V16>(A, L, T)
+                                           : cta_level<SC, D, V16>(A, L, T);
     if (!ok) return;
   }
 }
@@ -939,6 +1155,8 @@ template <int SC, int D> struct NodeSetSrc {
     const int j = level_of(i);
     return ((s + 1) << j) - 1 + (i - ((1 << j) - 1));
   }
+  int8_t *ancDim;
+  uint32_t *ancKey;
   template <class SM> __device__ void load(SM &S, int m) const
   {
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -947,7 +1165,23 @@ template <int SC, int D> struct NodeSetSrc {
       for (int d = 0; d < D; d++) S.key[d][i] = coord_key<SC>(R, node, d);
       S.idx[i] = R.idx ? R.idx[node] : uint32_t(node);
     }
-    if (explicitDims && threadIdx.x == 0) domain_box<SC, D>(R, wb, true, L0, s, S.rootLo, S.rootHi);
+    if (explicitDims) {
+      load_ancestors<SC, D>(R, true, L0, s, ancDim, ancKey);
+      if (threadIdx.x == 0) {
+        for (int d = 0; d < D; d++) {
+          S.rootLo[d] = wb[d];
+          S.rootHi[d] = wb[D + d];
+        }
+        for (int k = 0; k < L0; k++) {
+          const int64_t a = ((s + 1) >> (L0 - k)) - 1;
+          const int64_t c = ((s + 1) >> (L0 - k - 1)) - 1;
+          if (c == 2 * a + 1)
+            S.rootHi[ancDim[k]] = ancKey[k];
+          else
+            S.rootLo[ancDim[k]] = ancKey[k];
+        }
+      }
+    }
   }
   __device__ int anc_dim(int64_t a) const { return dim_at(R, a); }
   template <class SM> __device__ void settle(int64_t, int u, int piv, int, SM &) const
@@ -960,6 +1194,8 @@ template <int D> struct NodeSetSmem {
   SubSmem<D, kTile, kSubThreads> sub;
   uint16_t slotOf[kTile];
   uint32_t col[4][kTile];
+  int8_t ancDim[kMaxLevels];
+  uint32_t ancKey[kMaxLevels];
 };
 
 template <int SC, int D>
@@ -977,7 +1213,7 @@ __global__ void __launch_bounds__(kSubThreads, 3) subtree_kernel(Recs R, const u
   const int m = int(subtree_size(s, R.n));
   if (m == 0) return;
   for (int u = threadIdx.x; u < m; u += kSubThreads) S.slotOf[u] = uint16_t(u);
-  NodeSetSrc<SC, D> src{R, wb, s, L0, explicitDims, S.slotOf};
+  NodeSetSrc<SC, D> src{R, wb, s, L0, explicitDims, S.slotOf, S.ancDim, S.ancKey};
   build::subtree_body<SC, D, kTile, kSubThreads>(src, R.n, L0, s, explicitDims, S.sub);
   __syncthreads();
   // every node takes the record of its slot, four words at a time
@@ -1048,7 +1284,7 @@ __global__ void write_bounds_kernel(const uint32_t *wb, uint32_t *out)
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
-template <int SC, int D>
+template <int SC, int D, bool V16>
 int top_grid(int *grid)
 {
   static std::mutex mu;
@@ -1059,7 +1295,7 @@ int top_grid(int *grid)
   std::lock_guard<std::mutex> lock(mu);
   if (!cached[dev]) {
     int perSM = 0, sms = 0;
-    CKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, top_kernel<SC, D>, kThreads, 0));
+    CKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, top_kernel<SC, D, V16>, kThreads, 0));
     CKB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (perSM < 1) return CUKD_ERR_UNSUPPORTED;
     cached[dev] = perSM * sms;
@@ -1128,20 +1364,19 @@ int build_impl(void *pts, int64_t n, const Layout &L, void *worldBounds, cudaStr
       maxCh = std::max(maxCh, (int64_t(2) << lvl) * chunks_per_side(jmax, lc));
     }
     // once every spread level exists (n > 2^18) the scratch is the fixed
-    // maximum; smaller trees take less (a round pairs at most half the points)
+    // maximum; smaller trees take less
     const bool full = spreadLevels == build::ilog2_floor(kMultiSegs) + 1;
     if (full) maxCh = kMaxChunks;
     CKB_TRY(arena.alloc(&A.ccnt, maxCh));
     CKB_TRY(arena.alloc(&A.cst, maxCh));
-    A.npairs = full ? kPairs : std::min<int64_t>(kPairs, n / 2 + 1);
-    CKB_TRY(arena.alloc(&A.pairs, 2 * size_t(A.npairs)));
-    CKB_CUDA(cudaMemsetAsync(A.pairs, 0xff, sizeof(uint32_t) * 2 * size_t(A.npairs), st));
+    CKB_TRY(arena.alloc(&A.bnd, 2 * maxCh));
     CKB_CUDA(cudaMemsetAsync(A.hist, 0, sizeof(uint32_t) * size_t(nsegMax) * kBins, st));
+    const bool v16 = L.stride == 16 && (reinterpret_cast<uintptr_t>(pts) & 15) == 0;
     int grid = 0;
-    CKB_TRY((top_grid<SC, D>(&grid)));
+    CKB_TRY(v16 ? (top_grid<SC, D, true>(&grid)) : (top_grid<SC, D, false>(&grid)));
     void *args[] = {&A};
-    CKB_CUDA(cudaLaunchCooperativeKernel((const void *)top_kernel<SC, D>, dim3(grid), dim3(kThreads),
-                                         args, 0, st));
+    const void *fn = v16 ? (const void *)top_kernel<SC, D, true> : (const void *)top_kernel<SC, D, false>;
+    CKB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, st));
     count_launch();
   }
   {
