@@ -729,7 +729,8 @@ def reference_gpu_timings(recs, q):
             return a.elapsed_time(b)
 
         res = {}
-        for builder, name in ((0, "buildTree_thrust"), (1, "buildTree_bitonic")):
+        for builder, name in ((2, "buildTree_inPlace"), (1, "buildTree_bitonic"),
+                              (0, "buildTree_thrust")):
             ts = []
             for _ in range(2):
                 d.copy_(src)
@@ -737,6 +738,22 @@ def reference_gpu_timings(recs, q):
                                                      C.c_void_p(d.data_ptr()), n,
                                                      C.c_void_p(wb.data_ptr()))))
             res[name + "_ms"] = round(min(ts), 3)
+            if builder == 2:  # is its output a k-d tree? (checker only)
+                out = d.cpu().numpy().view(np.uint32).reshape(n, 4)
+                res["buildTree_inPlace_kd_violations"] = po.check_kd(
+                    out[:, :3].view(np.float32), (out[:, 3] >> 30).astype(np.int32),
+                    wb.cpu().numpy())
+        # where the reference's in-place builder's output is a valid tree:
+        # 10M uniform float2 / float4 points
+        from cudakdtree_b200 import workloads as wl
+        for code, D in ((po.REF_F2, 2), (po.REF_F4, 4)):
+            p = torch.from_numpy(wl.uniform_points(n, D, seed=7).astype(np.float32)).cuda()
+            wbD = torch.zeros((2, D), dtype=torch.float32, device="cuda")
+            res[f"buildTree_inPlace_uniform_float{D}_ms"] = round(timed(
+                lambda: L.refg_build(code, 2, C.c_void_p(p.data_ptr()), n,
+                                     C.c_void_p(wbD.data_ptr()))), 1)
+            res[f"buildTree_inPlace_uniform_float{D}_kd_violations"] = po.check_kd(p.cpu().numpy())
+            del p
         hb = np.ascontiguousarray(wb.cpu().numpy())
         knn = lambda: L.refg_knn(po.REF_F3_PACKED, 0, 0, K, C.c_void_p(d.data_ptr()), n,
                                  hb.ctypes.data_as(C.c_void_p), C.c_void_p(dq.data_ptr()), nq,
@@ -1119,20 +1136,46 @@ def kernel_case(name):
         q = torch.from_numpy(wl.gmm_points(10_000_000, seed=3, sample_seed=4)).cuda()
         for _ in range(2):
             ck.morton_order(q)
-    elif name == "build":  # the benchmark's 10M-point build
+    elif name in ("build", "inplace", "bitonic"):  # the benchmark's 10M-point build
         lay = ck.layout_for("float32", 3, stride=16, dim_offset=12, dim_shift=30, dim_bits=2)
         src = torch.from_numpy(wl.packed_records(wl.gmm_points(10_000_000, seed=3))
                                .view(np.int32).reshape(-1, 4).copy()).cuda()
         d = torch.empty_like(src)
         for _ in range(2):
             d.copy_(src)
-            ck.build_tree(d, layout=lay)
+            ck.build_tree(d, layout=lay, builder="default" if name == "build" else name)
+        ck.build_check()
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": name, "ok": True}))
 
 
 KERNEL_CASES = ("knn", "learned", "train", "infer", "heap", "fastint", "accumulate", "spatial",
-                "scatter", "build")
+                "scatter", "build", "inplace", "bitonic")
+
+
+def config_builders(ck, dev, peak=None):
+    """Every builder name on 10M uniform float2 / float3 / float4 points and
+    on the benchmark's 10M mixture records: build ms (fresh copy of the
+    input before each build, mean of three)."""
+    import torch
+    from cudakdtree_b200 import workloads as wl
+    timed = _timer()
+    out = {"config": "builders", "build_ms": {}}
+    cases = [(f"uniform10M_float{D}", torch.from_numpy(wl.uniform_points(10_000_000, D, seed=7)
+                                                      .astype(np.float32)).to(dev), None)
+             for D in (2, 3, 4)]
+    recs, _ = workload(N_POINTS, 1)
+    cases.append(("gmm10M_packed16", torch.from_numpy(recs.view(np.int32).reshape(-1, 4).copy())
+                  .to(dev), ck.layout_for("float32", 3, stride=RECORD_BYTES, dim_offset=12,
+                                          dim_shift=30, dim_bits=2)))
+    for name, src, lay in cases:
+        P = torch.empty_like(src)
+        copy = lambda: P.copy_(src)
+        for b in ("default", "bitonic", "inplace"):
+            out["build_ms"][f"{name}_{b}"] = round(timed(
+                lambda: ck.build_tree(P, layout=lay, builder=b), setup=copy), 3)
+        ck.build_check()
+    return out
 
 
 def run_configs(args):
@@ -1140,7 +1183,8 @@ def run_configs(args):
     import cudakdtree_b200 as ck
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    fns = {"c1": config_c1, "c2": config_c2, "c4": config_c4, "c5": config_c5}
+    fns = {"c1": config_c1, "c2": config_c2, "c4": config_c4, "c5": config_c5,
+           "builders": config_builders}
     peak, _ = measured_peaks()
     for name in [c.strip().lower() for c in args.configs.split(",") if c.strip()]:
         res = fns[name](ck, dev, peak)

@@ -113,8 +113,23 @@ typedef enum cukd_builder {
  * 2i+2), and -- for explicit-dim layouts -- writes each node's split dim
  * (the widest extent of its domain).  Writes the world bounds to
  * d_world_bounds when non-NULL (mandatory for explicit-dim layouts).
- * The output is the reference's canonical order (buildTree_host /
- * buildTree_thrust), ties included, whichever builder is named.
+ * Temporary memory (through `mem`) and output by builder:
+ *   DEFAULT, THRUST  ~65 bytes per point of float3; the reference's
+ *                    canonical order (buildTree_host / buildTree_thrust),
+ *                    ties included;
+ *   BITONIC          4 bytes per point (one uint32 tag, like the
+ *                    reference's) plus ~5.5 MB; the same canonical order;
+ *   INPLACE          ~5.5 MB whatever n (the reference's takes none); the
+ *                    canonical order whenever the coordinates decide every
+ *                    split (e.g. no two points share a coordinate value),
+ *                    otherwise a valid left-balanced k-d tree of the same
+ *                    records that depends only on the input array (the
+ *                    reference's builders promise no more with ties,
+ *                    testing/testBuildersSameResult.cu:96-99).
+ * BITONIC and INPLACE run one cooperative launch for the top levels; a
+ * bounded grid-barrier wait that gives up, or a failed consistency check,
+ * stops the build (cukd_build_check reports CUKD_ERR_TIMEOUT /
+ * CUKD_ERR_INTERNAL; the array then holds a permutation of its records).
  * Replaces cukd::buildTree (cukd/builder.h:108-152),
  * buildTree_thrust (cukd/builder_thrust.h:90-110),
  * buildTree_bitonic (cukd/builder_bitonic.h:83-94),
@@ -523,16 +538,19 @@ CUKD_API unsigned long long cukd_launch_count(void);
  * Synchronises the device.  No reference counterpart. */
 CUKD_API int cukd_async_wait_timeouts(unsigned int *count);
 
-/* Synchronises `stream` and returns CUKD_ERR_TIMEOUT if a bulk-copy wait of
+/* Synchronises `stream` and returns CUKD_ERR_TIMEOUT if a bounded wait of
  * a build on the current device gave up since the previous check (that
- * build stopped and left the caller's records exactly as they were), else
- * CUKD_OK.  The reference's builders synchronise and throw on failure
+ * build stopped; the default builder leaves the caller's records exactly as
+ * they were, the bitonic / in-place ones a permutation of them),
+ * CUKD_ERR_INTERNAL if a bitonic / in-place build's consistency check
+ * failed, else CUKD_OK.  The reference's builders synchronise and throw on failure
  * (builder_thrust.h:479-511, common.h:276-285); the C++ shim's buildTree
  * calls this after the build to do the same. */
 CUKD_API int cukd_build_check(cudaStream_t stream);
 
-/* Test hook: how many times the builder's first bulk-copy wait polls its
- * barrier before giving up, on the current device (default
+/* Test hook: how many times the builder's first bulk-copy wait, and the
+ * bitonic / in-place builders' grid barriers, poll before giving up, on the
+ * current device (default
  * CUKD_ASYNC_WAIT_POLLS_DEFAULT; 0 gives up at once, so that a test can make
  * the wait run out without any fault).  Synchronous. */
 #define CUKD_ASYNC_WAIT_POLLS_DEFAULT 4194304u
