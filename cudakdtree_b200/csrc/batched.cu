@@ -348,7 +348,7 @@ static int check_tuning(const cukd_batch_tuning &t)
 {
   if (t.build_tile != 512 && t.build_tile != 1024 && t.build_tile != 2048)
     return CUKD_ERR_INVALID_ARGUMENT;
-  if (t.block_size < 32 || t.block_size > 256 || t.block_size % 32) return CUKD_ERR_INVALID_ARGUMENT;
+  if (t.block_size < 32 || t.block_size > 512 || t.block_size % 32) return CUKD_ERR_INVALID_ARGUMENT;
   if (t.queries_per_thread != 1 && t.queries_per_thread != 2 && t.queries_per_thread != 4)
     return CUKD_ERR_INVALID_ARGUMENT;
   if (t.morton != 0 && t.morton != 1) return CUKD_ERR_INVALID_ARGUMENT;
@@ -429,8 +429,10 @@ static int query_impl(cukd_batch_plan_s *p, const float *pts, const float *bound
     QArgs b = a;
     b.order = p->fb_list;
     b.count_ptr = fa.fb_count;
+    b.block_size = std::min(b.block_size, 256);  // reference-order kernels: <= 256 threads
     return run_query(b, CUKD_FLOAT32, D, p->params.method, p->kind, st);
   }
+  a.block_size = std::min(a.block_size, 256);
   return run_query(a, CUKD_FLOAT32, D, p->params.method, p->kind, st);
 }
 
@@ -756,10 +758,15 @@ int cukd_batch_autotune(cukd_batch_plan *p, const float *d_points, const float *
   if (rc == CUKD_OK) rc = build_impl(p, p->tune_pts, p->d_bounds, st);
   // 2. query: Morton x block size x queries per thread
   float bestQuery = 3.4e38f;
-  const int sizes[3] = {64, 128, 256};
+  // 512-thread blocks only where the register-list kernel answers (k <= 32;
+  // the heap and reference-order kernels take at most 256)
+  const int sizes[4] = {64, 128, 256, 512};
+  const bool regList = !p->fcp && !(p->params.flags & (CUKD_QUERY_HEAP_ORDER | CUKD_QUERY_REFERENCE_ORDER)) &&
+                       p->params.k >= 2 && p->params.k <= 32;
+  const int nSizes = regList ? 4 : 3;
   const int qpts[3] = {1, 2, 4};
   for (int mo = 1; mo >= 0 && rc == CUKD_OK; mo--)
-    for (int bi = 0; bi < 3 && rc == CUKD_OK; bi++)
+    for (int bi = 0; bi < nSizes && rc == CUKD_OK; bi++)
       for (int qi = 0; qi < 3 && rc == CUKD_OK; qi++) {
         p->tuning.morton = mo;
         p->tuning.block_size = sizes[bi];

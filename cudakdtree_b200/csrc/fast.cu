@@ -42,12 +42,13 @@ namespace fast {
 using query::QArgs;
 using query::TreeView;
 
-// Register cap: at most 64 registers (4 resident 256-thread blocks per SM)
-// for lists of up to 17 slots in 2-D / 3-D (9 in 4-D), 128 otherwise.  The
+// Register cap: at most 64 registers (1024 resident threads per SM) for
+// lists of up to 17 slots in 2-D / 3-D (9 in 4-D), 128 otherwise.  The
 // kernel is latency-bound: the extra resident warps outweigh the few spilled
 // registers (measured 12% faster at k = 16 on the 10M-point benchmark).
+// Blocks of up to 512 threads (the batched path's autotuner tries 512).
 template <int D, bool EXPL, bool VEC16, int KC>
-__global__ void __launch_bounds__(256, ((KC <= 9 || (KC <= 17 && D <= 3)) ? 4 : 2))
+__global__ void __launch_bounds__(512, ((KC <= 9 || (KC <= 17 && D <= 3)) ? 2 : 1))
     knn_fast_kernel(FastArgs fa)
 {
   const int64_t limit = fa.q.count_ptr ? int64_t(*fa.q.count_ptr) : fa.q.nq;
@@ -242,7 +243,8 @@ __global__ void __launch_bounds__(256) knn_fast_heap_kernel(FastArgs fa)
 template <int D, bool EXPL, bool VEC16, int KH>
 int launch_fast_heap(const FastArgs &fa, cudaStream_t st)
 {
-  const int bs = fa.q.block_size > 0 ? fa.q.block_size : 128;
+  // the heap kernel takes blocks of at most 256 threads
+  const int bs = fa.q.block_size > 0 ? std::min(fa.q.block_size, 256) : 128;
   const int64_t grid = std::max<int64_t>(1, div_up(fa.q.nq, int64_t(bs)));
   knn_fast_heap_kernel<D, EXPL, VEC16, KH><<<unsigned(grid), bs, 0, st>>>(fa);
   CKB_CHECK_LAUNCH();

@@ -477,7 +477,8 @@ typedef struct cukd_batch_plan_s cukd_batch_plan;
 
 typedef struct cukd_batch_tuning {
   int32_t build_tile;          /* subtree-phase tile: 512, 1024 or 2048 points */
-  int32_t block_size;          /* query threads per block: 32..256, multiple of 32 */
+  int32_t block_size;          /* query threads per block: 32..512, multiple of 32
+                                * (above 256 only for k = 2..32 fixed lists) */
   int32_t queries_per_thread;  /* 1, 2 or 4 */
   int32_t morton;              /* 1: visit each cloud's queries in Morton order */
   float build_ms, query_ms;    /* cukd_batch_autotune: best times measured */

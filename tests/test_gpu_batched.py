@@ -138,6 +138,19 @@ def test_methods_and_k(method, k):
     _check(plan, pts, poff, qs, qoff, ref, bnd, built, got)
 
 
+@pytest.mark.parametrize("k", [0, 1, 40])
+def test_512_thread_blocks_where_other_kernels_answer(k):
+    """A 512-thread block tuning also where the heap kernel (k > 32) and the
+    reference-order kernels (FCP, k = 1, the exact fallbacks of tie-heavy
+    points) answer: those take at most 256 threads and are launched so."""
+    pts, poff, qs, qoff = _clouds(EDGE_SIZES, 3, "tie", seed=40 + k)
+    ref = _oracle(pts, poff, qs, qoff, k, po.STACK_BASED)
+    plan = ck.BatchPlan(poff, qoff, 3, k=k)
+    plan.set_tuning(block_size=512, queries_per_thread=2)
+    built, bnd, got = _run_build_query(plan, pts, qs)
+    _check(plan, pts, poff, qs, qoff, ref, bnd, built, got)
+
+
 def test_cutoff_radius():
     pts, poff, qs, qoff = _clouds(EDGE_SIZES, 3, "uniform", seed=3)
     ref = _oracle(pts, poff, qs, qoff, 8, po.STACK_BASED, cutoff=0.05)
@@ -146,7 +159,8 @@ def test_cutoff_radius():
     _check(plan, pts, poff, qs, qoff, ref, bnd, built, got)
 
 
-@pytest.mark.parametrize("block,qpt,morton", [(32, 1, 1), (64, 4, 0), (256, 2, 1), (128, 1, 0)])
+@pytest.mark.parametrize("block,qpt,morton", [(32, 1, 1), (64, 4, 0), (256, 2, 1), (128, 1, 0),
+                                             (512, 1, 1), (512, 4, 0)])
 def test_query_tunings_same_answers(block, qpt, morton):
     pts, poff, qs, qoff = _clouds(EDGE_SIZES, 3, "uniform", seed=9)
     ref = _oracle(pts, poff, qs, qoff, 8, po.STACK_BASED)
@@ -188,7 +202,7 @@ def test_autotune_keeps_points_and_answers():
     torch.cuda.synchronize()
     assert np.array_equal(f32_bits(P.cpu().numpy()), f32_bits(pts))
     assert t.build_tile in (512, 1024, 2048)
-    assert t.block_size in (64, 128, 256) and t.queries_per_thread in (1, 2, 4)
+    assert t.block_size in (64, 128, 256, 512) and t.queries_per_thread in (1, 2, 4)
     assert t.morton in (0, 1) and t.build_ms > 0 and t.query_ms > 0
     assert plan.tuning.as_dict() == t.as_dict()
     bnd = plan.bounds_tensor(P.device)
@@ -207,6 +221,8 @@ def test_invalid_arguments():
         plan.set_tuning(build_tile=4096)
     with pytest.raises(ck.CukdError):
         plan.set_tuning(block_size=48)
+    with pytest.raises(ck.CukdError):
+        plan.set_tuning(block_size=544)
     with pytest.raises(ck.CukdError):
         ck.BatchPlan(np.array([0, 10]), np.array([0, 4]), 5, k=8)
 
