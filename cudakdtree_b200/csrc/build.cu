@@ -114,9 +114,9 @@ __device__ uint32_t g_wait_polls = kWaitPolls;
 constexpr int kBinPoints = 32;  // target points per histogram bin (global levels)
 
 struct Bufs {
-  uint32_t *key[2][4];
+  uint32_t *key[2][kMaxDims];
   uint32_t *idx[2];
-  uint32_t *ckey[4];
+  uint32_t *ckey[kMaxDims];
   uint32_t *cidx;
   uint32_t *perm;  // node -> input index
   uint8_t *ndim;   // node -> split dim
@@ -1753,8 +1753,9 @@ int build_dispatch(void *pts, int64_t n, const Layout &L, void *wb, cudaStream_t
   using namespace build;
 #define CKB_CASE(SC_, D_) \
   if (L.scalar == SC_ && L.D == D_) return build_impl<SC_, D_>(pts, n, L, wb, st, mem);
-  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
-  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4) CKB_CASE(0, 5) CKB_CASE(0, 6) CKB_CASE(0, 7)
+  CKB_CASE(0, 8) CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4) CKB_CASE(1, 5) CKB_CASE(1, 6)
+  CKB_CASE(1, 7) CKB_CASE(1, 8)
 #undef CKB_CASE
   return CUKD_ERR_UNSUPPORTED;
 }
@@ -1764,8 +1765,9 @@ int bounds_dispatch(const void *pts, int64_t n, const Layout &L, void *out, cuda
   using namespace build;
 #define CKB_CASE(SC_, D_) \
   if (L.scalar == SC_ && L.D == D_) return bounds_impl<SC_, D_>(pts, n, L, out, st);
-  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
-  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4) CKB_CASE(0, 5) CKB_CASE(0, 6) CKB_CASE(0, 7)
+  CKB_CASE(0, 8) CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4) CKB_CASE(1, 5) CKB_CASE(1, 6)
+  CKB_CASE(1, 7) CKB_CASE(1, 8)
 #undef CKB_CASE
   return CUKD_ERR_UNSUPPORTED;
 }

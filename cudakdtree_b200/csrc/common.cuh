@@ -182,6 +182,14 @@ __host__ __device__ inline int64_t seg_begin(int64_t g, int lvl, int64_t n)
 // ---------------------------------------------------------------------------
 // record access
 // ---------------------------------------------------------------------------
+// points of up to 8 dims (the reference's vec_float<N>, cukd-math.h:133-181,
+// tested up to N = 8 in testing/testBuildersSameResult.cu:404-428) build with
+// every builder and answer through the reference-order traversals; the fast
+// kNN, learned, spatial, batched, Morton and allocation-free paths take up
+// to 4
+constexpr int kMaxDims = 8;
+constexpr int kMaxFastDims = 4;
+
 struct Layout {
   int scalar, D, stride, poff, doff, dshift;
   uint32_t dmask;
@@ -190,7 +198,7 @@ inline bool make_layout(const cukd_layout *l, Layout *out)
 {
   if (!l) return false;
   if (l->scalar_type != CUKD_FLOAT32 && l->scalar_type != CUKD_INT32) return false;
-  if (l->num_dims < 2 || l->num_dims > 4) return false;
+  if (l->num_dims < 2 || l->num_dims > kMaxDims) return false;
   if (l->stride <= 0 || (l->stride & 3) || (l->point_offset & 3) || l->point_offset < 0) return false;
   if (l->point_offset + 4 * l->num_dims > l->stride) return false;
   out->scalar = l->scalar_type;

@@ -81,7 +81,7 @@ static_assert(kPerThread * kThreads == kBins, "bins per thread");
 constexpr int kMultiSegs = 128;
 // record words the in-place tie-break compares after the coordinates
 constexpr int kMaxRaw = 60;
-constexpr int kMaxWords = 4 + kMaxRaw;
+constexpr int kMaxWords = kMaxDims + kMaxRaw;
 constexpr int kMaxChunks = 1 << 17;  // chunks of a spread level
 constexpr int kMinChunkLog = 12;     // chunks of at least 4096 points
 constexpr int kQueue = 4096;         // ring of misplaced positions, per side
@@ -1398,8 +1398,9 @@ int inplace_dispatch(void *pts, int64_t n, const Layout &L, void *wb, cudaStream
   using namespace inplace;
 #define CKB_CASE(SC_, D_) \
   if (L.scalar == SC_ && L.D == D_) return build_impl<SC_, D_>(pts, n, L, wb, st, mem, bitonic);
-  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
-  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4) CKB_CASE(0, 5) CKB_CASE(0, 6) CKB_CASE(0, 7)
+  CKB_CASE(0, 8) CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4) CKB_CASE(1, 5) CKB_CASE(1, 6)
+  CKB_CASE(1, 7) CKB_CASE(1, 8)
 #undef CKB_CASE
   return CUKD_ERR_UNSUPPORTED;
 }

@@ -176,8 +176,9 @@ int run_query(const QArgs &a, int scalar, int D, int method, int kind, cudaStrea
 {
 #define CKB_CASE(SC_, D_) \
   if (scalar == SC_ && D == D_) return dispatch_layout<SC_, D_>(a, method, kind, st);
-  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4)
-  CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4)
+  CKB_CASE(0, 2) CKB_CASE(0, 3) CKB_CASE(0, 4) CKB_CASE(0, 5) CKB_CASE(0, 6) CKB_CASE(0, 7)
+  CKB_CASE(0, 8) CKB_CASE(1, 2) CKB_CASE(1, 3) CKB_CASE(1, 4) CKB_CASE(1, 5) CKB_CASE(1, 6)
+  CKB_CASE(1, 7) CKB_CASE(1, 8)
 #undef CKB_CASE
   return CUKD_ERR_UNSUPPORTED;
 }
@@ -237,7 +238,9 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   a.visits = visits;
   a.block_size = p->block_size;
   TempArena arena(st, mem);
-  if ((p->flags & CUKD_QUERY_TREE_ORDER) && nq > 1 && n > 0) {
+  // query orders (tree path, Morton) and the fast path: up to 4 dims
+  const bool narrow = L.D <= kMaxFastDims;
+  if ((p->flags & CUKD_QUERY_TREE_ORDER) && nq > 1 && n > 0 && narrow) {
     uint32_t *codes = nullptr, *codes2 = nullptr, *vals = nullptr, *vals2 = nullptr;
     CKB_TRY(arena.alloc(&codes, nq));
     CKB_TRY(arena.alloc(&codes2, nq));
@@ -247,7 +250,7 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
     CKB_TRY(run_tree_path(a, L.scalar, L.D, levels, codes, vals, st));
     CKB_TRY(radix_sort_pairs(codes, vals, codes2, vals2, nq, levels, st, &arena));
     a.order = (const int32_t *)vals;
-  } else if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32) {
+  } else if ((p->flags & CUKD_QUERY_MORTON) && nq > 1 && L.scalar == CUKD_FLOAT32 && narrow) {
     int32_t *perm = nullptr;
     CKB_TRY(arena.alloc(&perm, nq));
     // the Morton grid spans the tree's world bounds when the caller passes
@@ -260,7 +263,7 @@ static int common_query(const void *d_tree, int64_t n, const cukd_layout *layout
   // fast exact path (see fast.cu): any visiting order, boundary-tie check,
   // reference-order re-run of the queued queries
   const bool fastOk = !visits && !a.heap_order && !(p->flags & CUKD_QUERY_REFERENCE_ORDER) &&
-                      knn && p->k >= 2 && p->k <= 128 && n < (int64_t(1) << 31) - 1;
+                      knn && p->k >= 2 && p->k <= 128 && n < (int64_t(1) << 31) - 1 && narrow;
   // (FCP and k = 1 stay on the reference traversals: with a single
   // candidate the split-plane bound is already cheap and the corner
   // bookkeeping does not pay for itself)

@@ -33,8 +33,8 @@ template <typename point_t> struct ShimRecord {
 template <typename point_t> inline cukd_layout layout_of(int stride, int dim_offset)
 {
   using S = typename point_traits<point_t>::scalar_t;
-  static_assert(point_traits<point_t>::num_dims >= 2 && point_traits<point_t>::num_dims <= 4,
-                "cukd-b200 builds trees over 2, 3 or 4 dimensions");
+  static_assert(point_traits<point_t>::num_dims >= 2 && point_traits<point_t>::num_dims <= 8,
+                "cukd-b200 builds trees over 2 to 8 dimensions");
   static_assert(std::is_same<S, float>::value || std::is_same<S, int>::value,
                 "cukd-b200 builds trees over float or int coordinates");
   cukd_layout l;

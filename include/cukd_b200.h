@@ -76,7 +76,12 @@ typedef enum cukd_scalar_type { CUKD_FLOAT32 = 0, CUKD_INT32 = 1 } cukd_scalar_t
 
 typedef struct cukd_layout {
   int32_t scalar_type;  /* cukd_scalar_type */
-  int32_t num_dims;     /* 2, 3 or 4 */
+  int32_t num_dims;     /* 2..8 (the reference's float2/3/4, int2/3/4 and
+                         * vec_float<N>); every builder and the reference-order
+                         * FCP / kNN take up to 8, the fast kNN, learned radius,
+                         * spatial tree, batched plans, Morton order and the
+                         * allocation-free builder up to 4 (else
+                         * CUKD_ERR_UNSUPPORTED / INVALID_ARGUMENT) */
   int32_t stride;       /* bytes per record, multiple of 4 */
   int32_t point_offset; /* byte offset of coordinate 0, multiple of 4 */
   int32_t dim_offset;   /* byte offset of the dim word, multiple of 4; -1 = none */

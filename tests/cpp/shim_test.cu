@@ -50,6 +50,17 @@ template <typename T> static void dump(const std::string &path, const std::vecto
   fclose(f);
 }
 
+// 8-dim points, the reference's own vec_float<N> (cukd-math.h:133-181)
+using Vec8 = cukd::vec_float<8>;
+__global__ void knn8_vec8(const Vec8 *tree, int n, const Vec8 *q, int nq, int *ids)
+{
+  const int i = threadIdx.x + blockIdx.x * blockDim.x;
+  if (i >= nq) return;
+  cukd::FixedCandidateList<8> result(INFINITY);
+  cukd::stackBased::knn<cukd::FixedCandidateList<8>, Vec8>(result, q[i], tree, n);
+  for (int j = 0; j < 8; j++) ids[i * 8 + j] = result.get_pointID(j);
+}
+
 __global__ void knn8(const PointPlusPayload *tree, int n, const float3 *q, int nq, int *ids,
                      float *d2)
 {
@@ -257,6 +268,41 @@ int main(int argc, char **argv)
     }
     cudaFree(d);
     cudaFree(res);
+  }
+  // 6) vec_float<8>: the reference builder test's N = 8 inputs (unique
+  //    integer coordinates, scrambled), buildTree and a user kNN kernel
+  {
+    const int m = 10000, mq = 2000;
+    std::vector<int> u(m * 8);
+    for (int i = 0; i < m * 8; i++) u[i] = i;
+    std::mt19937 g8(88);
+    for (int i = m * 8 - 1; i > 0; --i) std::swap(u[i], u[std::uniform_int_distribution<>(0, i)(g8)]);
+    std::vector<Vec8> p8(m), q8(mq);
+    for (int i = 0; i < m; i++)
+      for (int d = 0; d < 8; d++) p8[i].v[d] = float(u[i * 8 + d]);
+    std::uniform_real_distribution<float> U8(0.f, float(m * 8));
+    for (auto &q : q8)
+      for (int d = 0; d < 8; d++) q.v[d] = U8(g8);
+    dump(out + "/vec8_points.bin", p8);
+    dump(out + "/vec8_queries.bin", q8);
+    Vec8 *d, *dq;
+    int *ids;
+    CUKD_CUDA_CALL(Malloc(&d, sizeof(Vec8) * m));
+    CUKD_CUDA_CALL(Malloc(&dq, sizeof(Vec8) * mq));
+    CUKD_CUDA_CALL(Malloc(&ids, sizeof(int) * mq * 8));
+    CUKD_CUDA_CALL(Memcpy(d, p8.data(), sizeof(Vec8) * m, cudaMemcpyHostToDevice));
+    CUKD_CUDA_CALL(Memcpy(dq, q8.data(), sizeof(Vec8) * mq, cudaMemcpyHostToDevice));
+    cukd::buildTree<Vec8>(d, m);
+    knn8_vec8<<<(mq + 127) / 128, 128>>>(d, m, dq, mq, ids);
+    CUKD_CUDA_SYNC_CHECK();
+    CUKD_CUDA_CALL(Memcpy(p8.data(), d, sizeof(Vec8) * m, cudaMemcpyDeviceToHost));
+    std::vector<int> hi(mq * 8);
+    CUKD_CUDA_CALL(Memcpy(hi.data(), ids, sizeof(int) * mq * 8, cudaMemcpyDeviceToHost));
+    dump(out + "/vec8_tree.bin", p8);
+    dump(out + "/vec8_knn8.bin", hi);
+    cudaFree(d);
+    cudaFree(dq);
+    cudaFree(ids);
   }
   printf("shim_test OK\n");
   return 0;

@@ -47,7 +47,7 @@ def test_invalid_layouts_are_rejected_before_any_device_work():
     import ctypes as C
     import cudakdtree_b200 as ck
     L = ck.lib()
-    bad = [ck.layout_for("float32", 5), ck.layout_for("float32", 3, stride=10),
+    bad = [ck.layout_for("float32", 9), ck.layout_for("float32", 1), ck.layout_for("float32", 3, stride=10),
            ck.layout_for("float32", 3, stride=16, point_offset=8),
            ck.layout_for("float32", 3, stride=16, dim_offset=14),
            ck.layout_for("float32", 4, stride=20, dim_offset=16, dim_shift=31, dim_bits=1)]

@@ -64,3 +64,17 @@ def test_spatial_tree_user_kernel(out):
     nodes, prims, b = po.spatial_build(pts)
     ri, _ = po.spatial_knn(nodes, prims, pts, b, q, 16, po.CCT, list_kind=po.HEAP_LIST)
     assert np.array_equal(_f(out, "spatial_knn16.bin", np.int32, 16), ri)
+
+
+def test_vec_float8_build_and_user_knn_kernel(out):
+    """cukd::buildTree<cukd::vec_float<8>> on the reference builder test's
+    N = 8 inputs (unique integer coordinates,
+    testing/testBuildersSameResult.cu:404-428) and a user kNN kernel
+    (stackBased::knn<FixedCandidateList<8>, vec_float<8>>) over the tree."""
+    pts = _f(out, "vec8_points.bin", np.float32, 8)
+    q = _f(out, "vec8_queries.bin", np.float32, 8)
+    perm, _, bounds = po.build(pts)
+    tree = _f(out, "vec8_tree.bin", np.float32, 8)
+    assert np.array_equal(tree, pts[perm])
+    ri, _, _ = po.knn(pts[perm], q, 8, po.STACK_BASED, bounds=bounds)
+    assert np.array_equal(_f(out, "vec8_knn8.bin", np.int32, 8), ri)
