@@ -952,6 +952,11 @@ def config_c4(ck, dev, peak):
             "learned_queries_per_s": round(nq / (t_learned / 1e3), 1),
             "learned_speedup_vs_plain": round(t_plain / t_learned, 3),
             "plain_knn_frac": _frac(kb, t_plain, peak),
+            "plain_knn_mean_visits_ref": round(mv, 2),
+            "plain_knn_frac_note": "algorithmic bytes = reference stack-based visits x 16 B + "
+                                   "query + answers: the uniform 30% of the queries, far from "
+                                   "the mixture, make the reference order visit many nodes "
+                                   "that corner culling skips, so the fraction exceeds 1",
             "fallback_rate": round(int(fb[0][0].item()) / nq, 5),
             "identical_results": same, "clocks": clocks}
 
