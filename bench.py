@@ -743,6 +743,18 @@ def reference_gpu_timings(recs, q):
                 res["buildTree_inPlace_kd_violations"] = po.check_kd(
                     out[:, :3].view(np.float32), (out[:, 3] >> 30).astype(np.int32),
                     wb.cpu().numpy())
+        # the reference's spatial k-d tree builder on the same points (float3)
+        pts3 = torch.from_numpy(np.ascontiguousarray(
+            recs.view(np.float32).reshape(n, 4)[:, :3])).cuda()
+        ms = C.c_float(0.0)
+        sp = []
+        for _ in range(2):
+            if L.refg_spatial_build_ms_float3(C.c_void_p(pts3.data_ptr()), n, 8,
+                                              C.byref(ms)) != 0:
+                raise RuntimeError("reference spatial build failed")
+            sp.append(ms.value)
+        res["spatial_buildTree_ms"] = round(min(sp), 3)
+        del pts3
         # where the reference's in-place builder's output is a valid tree:
         # 10M uniform float2 / float4 points
         from cudakdtree_b200 import workloads as wl

@@ -110,6 +110,7 @@ def ref_gpu():
         L.refg_knn.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P, _P, C.c_int,
                                C.c_float, _P, _P]
         L.refg_spatial_build_float3.argtypes = [_P, C.c_int, C.c_int, _P, _P, _P, _P]
+        L.refg_spatial_build_ms_float3.argtypes = [_P, C.c_int, C.c_int, _P]
         _ref_gpu = L
     return _ref_gpu
 

@@ -161,4 +161,25 @@ int refg_spatial_build_float3(const void *d_pts, int n, int leaf_threshold, void
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
 
+// The same build timed alone (CUDA events around the reference's buildTree
+// call, its own allocations included), the tree freed afterwards.
+int refg_spatial_build_ms_float3(const void *d_pts, int n, int leaf_threshold, float *ms)
+{
+  cukd::SpatialKDTree<float3> tree;
+  cukd::BuildConfig cfg;
+  cfg.makeLeafThreshold = leaf_threshold;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, 0);
+  cukd::buildTree(tree, (float3 *)d_pts, n, cfg);
+  cudaEventRecord(b, 0);
+  const bool ok = cudaEventSynchronize(b) == cudaSuccess;
+  cudaEventElapsedTime(ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cukd::free(tree);
+  return ok && cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
 }  // extern "C"
