@@ -369,24 +369,40 @@ def run_ours(args, rank, world, local):
         # search overlap the device->host copy of the previous step's answers
         # (PCIe copies both ways at once; the answers, 1.28 GB, are the
         # slowest stage)
-        lanes = []
+        # one compute stream (the current one) runs each step's build and
+        # search back to back; the next step's points go up on a side stream
+        # once its tree buffer is free; each step's answers land behind its
+        # own event (cukd_knn_host_async), so the device->host copies of one
+        # step overlap the compute of the next
+        up_stream = torch.cuda.Stream()
+        slots = []
         for j in range(2):
-            lanes.append({"stream": torch.cuda.Stream(),
-                          "pts": d_pts if j == 0 else torch.empty_like(d_pts),
+            slots.append({"pts": d_pts if j == 0 else torch.empty_like(d_pts),
                           "wb": wb if j == 0 else torch.empty_like(wb),
                           "ids": h_ids if j == 0 else torch.empty_like(h_ids).pin_memory(),
-                          "d2": h_d2 if j == 0 else torch.empty_like(h_d2).pin_memory()})
+                          "d2": h_d2 if j == 0 else torch.empty_like(h_d2).pin_memory(),
+                          "done": torch.cuda.Event(), "free": torch.cuda.Event(),
+                          "up": torch.cuda.Event(), "used": False})
         step_no = [0]
 
         def pipelined_step():
-            ln = lanes[step_no[0] % 2]
+            sl = slots[step_no[0] % 2]
             step_no[0] += 1
-            with torch.cuda.stream(ln["stream"]):
-                ln["pts"].copy_(h_pts, non_blocking=True)
-                ck.build_tree(ln["pts"], layout=lay, world_bounds=ln["wb"])
-                ck.knn_host(ln["pts"], h_q, K, "stack_based", layout=lay,
-                            world_bounds=ln["wb"], out_ids=ln["ids"], out_d2=ln["d2"],
-                            chunk=args.e2e_chunk)
+            main = torch.cuda.current_stream()
+            if sl["used"]:
+                up_stream.wait_event(sl["free"])  # the search two steps back has run
+            with torch.cuda.stream(up_stream):
+                sl["pts"].copy_(h_pts, non_blocking=True)
+            sl["up"].record(up_stream)
+            main.wait_event(sl["up"])
+            if sl["used"]:
+                main.wait_event(sl["done"])  # its host buffers: that step's answers landed
+            ck.build_tree(sl["pts"], layout=lay, world_bounds=sl["wb"])
+            ck.knn_host(sl["pts"], h_q, K, "stack_based", layout=lay, world_bounds=sl["wb"],
+                        out_ids=sl["ids"], out_d2=sl["d2"], chunk=args.e2e_chunk,
+                        done=sl["done"])
+            sl["free"].record(main)
+            sl["used"] = True
 
         def timed_pipelined():
             for _ in range(2):
@@ -395,12 +411,10 @@ def run_ours(args, rank, world, local):
             main = torch.cuda.current_stream()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(main)
-            for ln in lanes:
-                ln["stream"].wait_event(a)
             for _ in range(args.steps):
                 pipelined_step()
-            for ln in lanes:
-                main.wait_stream(ln["stream"])
+            for sl in slots:
+                main.wait_event(sl["done"])
             b.record(main)
             barrier()
             return max_over_ranks(a.elapsed_time(b), pg, dev) / args.steps
@@ -440,7 +454,7 @@ def run_ours(args, rank, world, local):
         et = timed_pipelined()
         st_ms = timed(e2e_step)
         dt = timed(device_queries_step)
-        lanes[1]["pts"] = lanes[1]["ids"] = lanes[1]["d2"] = None
+        slots[1]["pts"] = slots[1]["ids"] = slots[1]["d2"] = None
 
         # the PCIe copies alone (one whole-array copy each way, pinned host
         # memory): the floor under any e2e step that moves these bytes
@@ -466,10 +480,11 @@ def run_ours(args, rank, world, local):
                "d2h_bytes_per_step": int(h_ids.numel() * 4 + h_d2.numel() * 4),
                "ms_per_step": round(et, 3),
                "pcie_copies_alone_ms": {"h2d": round(up_ms, 3), "d2h": round(down_ms, 3)},
-               "api": (f"cukd_build_tree + cukd_knn_host (pinned host queries and results, "
-                       f"{args.e2e_chunk}-query chunks on overlapping copy / search streams), "
-                       "two steps in flight on two streams with their own device tree and "
-                       "answer buffers"),
+               "api": (f"cukd_build_tree + cukd_knn_host_async (pinned host queries and "
+                       f"results, {args.e2e_chunk}-query chunks on overlapping copy / search "
+                       "streams) on one stream, each step's answers landing behind its own "
+                       "event while the next step builds and searches; the next step's points "
+                       "uploaded on a side stream; two device trees and answer buffers"),
                "one_step_at_a_time": {
                    "value": round(whole_job_rate(nq, world, st_ms), 1),
                    "ms_per_step": round(st_ms, 3),

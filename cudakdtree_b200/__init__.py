@@ -358,10 +358,13 @@ def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, 
 
 def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
              cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, out_ids=None, out_d2=None,
-             chunk=0, stream=None):
+             chunk=0, stream=None, done=None):
     """knn() with host-resident queries and results (CPU tensors; pin them
     for the copies to overlap the search).  Returns (ids, d2) CPU tensors,
-    complete once ``stream`` (default: the current stream) is synchronised."""
+    complete once ``stream`` (default: the current stream) is synchronised --
+    or, with ``done`` (a torch.cuda.Event), once that event has completed,
+    the stream being free as soon as the searches are queued
+    (cukd_knn_host_async)."""
     layout = layout or infer_layout(tree)
     if n is None:
         n = _num_records(tree, layout)
@@ -375,6 +378,20 @@ def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=N
                                                           pin_memory=pin)
     d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, pin_memory=pin)
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
+    if done is not None:
+        if not done.cuda_event:  # created lazily by torch: record once to create it
+            done.record(stream if isinstance(stream, torch.cuda.Stream)
+                        else torch.cuda.current_stream())
+        L = lib()
+        L.cukd_knn_host_async.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Layout), C.c_void_p,
+                                          C.c_void_p, C.c_int64, C.POINTER(QueryParams),
+                                          C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]
+        _check(L.cukd_knn_host_async(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                                     _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2),
+                                     int(chunk), C.c_void_p(done.cuda_event), _stream(stream),
+                                     None), "cukd_knn_host_async")
+        return ids, d2
     _check(lib().cukd_knn_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds), _ptr(queries),
                                nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk), _stream(stream),
                                None), "cukd_knn_host")

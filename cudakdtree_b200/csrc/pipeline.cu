@@ -15,6 +15,14 @@
 // whose queries and answers live in host memory (the reference's samples
 // copy whole arrays with cudaMemcpy around one query launch,
 // sample.cu:121-160); results are those of cukd_knn.
+//   cukd_knn_host_async  cukd_knn_host that leaves the caller's stream free
+//                     once the searches are queued: the answers land behind
+//                     the caller's event `done` (the result buffers, up to
+//                     eight sets, are released on the copy stream), so a
+//                     caller can queue the next tree's build and search on
+//                     the same stream while these answers are still being
+//                     copied -- the compute and the device->host copies of
+//                     consecutive batches then overlap.
 #include <algorithm>
 
 #include "common.cuh"
@@ -27,15 +35,16 @@ extern "C" int cukd_knn(const void *d_tree, int64_t n, const cukd_layout *layout
 namespace ckb {
 namespace {
 
-constexpr int kSets = 3;  // device buffer sets (queries, ids, d2)
+constexpr int kSets = 3;     // device buffer sets (queries, ids, d2)
+constexpr int kMaxSets = 8;  // ... when the copies do not hold the caller's stream
 
 struct PipeRes {
   cudaStream_t up = nullptr, down = nullptr;
-  cudaEvent_t upDone[kSets] = {}, searchDone[kSets] = {}, downDone[kSets] = {};
+  cudaEvent_t upDone[kMaxSets] = {}, searchDone[kMaxSets] = {}, downDone[kMaxSets] = {};
   cudaEvent_t start = nullptr, join[2] = {};
   ~PipeRes()
   {
-    for (int i = 0; i < kSets; i++) {
+    for (int i = 0; i < kMaxSets; i++) {
       if (upDone[i]) cudaEventDestroy(upDone[i]);
       if (searchDone[i]) cudaEventDestroy(searchDone[i]);
       if (downDone[i]) cudaEventDestroy(downDone[i]);
@@ -49,19 +58,26 @@ struct PipeRes {
 };
 
 // On every exit, success or error: the caller's stream waits for all work
-// queued on the side streams, so that the buffers released on it afterwards
-// (stream-ordered) are no longer in use.
+// queued on the side streams (only the upload stream when the answers land
+// behind the caller's event instead), so that the buffers released on it
+// afterwards (stream-ordered) are no longer in use.
 struct JoinSideStreams {
   PipeRes &r;
   cudaStream_t stream;
+  bool down = true;
   ~JoinSideStreams()
   {
-    cudaStream_t side[2] = {r.up, r.down};
+    cudaStream_t side[2] = {r.up, down ? r.down : nullptr};
     for (int i = 0; i < 2; i++) {
       if (!side[i] || !r.join[i]) continue;
       if (cudaEventRecord(r.join[i], side[i]) == cudaSuccess)
         cudaStreamWaitEvent(stream, r.join[i], 0);
     }
+    // the other way round when the result buffers are released on the copy
+    // stream: after every search queued on the caller's stream (also on an
+    // error midway, when some search has no copy behind it)
+    if (!down && r.down && r.join[1] && cudaEventRecord(r.join[1], stream) == cudaSuccess)
+      cudaStreamWaitEvent(r.down, r.join[1], 0);
   }
 };
 
@@ -77,7 +93,8 @@ namespace {
 int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
                  const void *d_world_bounds, const void *h_queries, const void *d_queries,
                  int64_t nq, const cukd_query_params *params, int32_t *h_out_ids, void *h_out_d2,
-                 int64_t chunk, cudaStream_t stream, const cukd_mem_resource *mem)
+                 int64_t chunk, cudaStream_t stream, const cukd_mem_resource *mem,
+                 cudaEvent_t done = nullptr)
 {
   Layout L;
   if (!make_layout(layout, &L) || !params) return CUKD_ERR_INVALID_ARGUMENT;
@@ -97,7 +114,9 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
     set_cuda_error(cudaGetLastError());
     return CUKD_ERR_CUDA;
   }
-  for (int i = 0; i < kSets; i++) {
+  const int64_t chunks = div_up(nq, chunk);
+  const int sets = done ? int(std::min<int64_t>(kMaxSets, chunks)) : kSets;
+  for (int i = 0; i < sets; i++) {
     CKB_CUDA(cudaEventCreateWithFlags(&r.upDone[i], cudaEventDisableTiming));
     CKB_CUDA(cudaEventCreateWithFlags(&r.searchDone[i], cudaEventDisableTiming));
     CKB_CUDA(cudaEventCreateWithFlags(&r.downDone[i], cudaEventDisableTiming));
@@ -106,36 +125,38 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
   for (cudaEvent_t &e : r.join) CKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
   TempArena arena(stream, mem);
-  uint8_t *dq[kSets] = {};
-  int32_t *di[kSets];
-  uint8_t *dd[kSets] = {};
-  for (int b = 0; b < kSets; b++) {
+  // the result buffers: released on the copy stream when the answers land
+  // behind `done` (after the copies), else on the caller's stream
+  TempArena downArena(done ? r.down : stream, mem);
+  uint8_t *dq[kMaxSets] = {};
+  int32_t *di[kMaxSets];
+  uint8_t *dd[kMaxSets] = {};
+  for (int b = 0; b < sets; b++) {
     if (upload) CKB_TRY(arena.alloc(&dq[b], size_t(chunk * qBytes)));
-    CKB_TRY(arena.alloc(&di[b], size_t(chunk * k)));
-    if (h_out_d2) CKB_TRY(arena.alloc(&dd[b], size_t(chunk * k * d2Bytes)));
+    CKB_TRY(downArena.alloc(&di[b], size_t(chunk * k)));
+    if (h_out_d2) CKB_TRY(downArena.alloc(&dd[b], size_t(chunk * k * d2Bytes)));
   }
-  // declared after the arena: joins the side streams before it releases
-  JoinSideStreams joiner{r, stream};
+  // declared after the arenas: joins the side streams before they release
+  JoinSideStreams joiner{r, stream, done == nullptr};
   // the side streams start after the work already queued on `stream`
   CKB_CUDA(cudaEventRecord(r.start, stream));
   if (upload) CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
   CKB_CUDA(cudaStreamWaitEvent(r.down, r.start, 0));
-  const int64_t chunks = div_up(nq, chunk);
   for (int64_t c = 0; c < chunks; c++) {
-    const int b = int(c % kSets);
+    const int b = int(c % sets);
     const int64_t q0 = c * chunk, m = std::min(chunk, nq - q0);
     const void *qs = (const uint8_t *)d_queries + q0 * qBytes;
     if (upload) {
-      // query buffer b: free once the search of chunk c - kSets has run
-      if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(r.up, r.searchDone[b], 0));
+      // query buffer b: free once the search of chunk c - sets has run
+      if (c >= sets) CKB_CUDA(cudaStreamWaitEvent(r.up, r.searchDone[b], 0));
       CKB_CUDA(cudaMemcpyAsync(dq[b], (const uint8_t *)h_queries + q0 * qBytes,
                                size_t(m * qBytes), cudaMemcpyHostToDevice, r.up));
       CKB_CUDA(cudaEventRecord(r.upDone[b], r.up));
       CKB_CUDA(cudaStreamWaitEvent(stream, r.upDone[b], 0));
       qs = dq[b];
     }
-    // result buffers b: free once chunk c - kSets' answers are copied down
-    if (c >= kSets) CKB_CUDA(cudaStreamWaitEvent(stream, r.downDone[b], 0));
+    // result buffers b: free once chunk c - sets' answers are copied down
+    if (c >= sets) CKB_CUDA(cudaStreamWaitEvent(stream, r.downDone[b], 0));
     CKB_TRY(cukd_knn(d_tree, n, layout, d_world_bounds, qs, m, params, di[b], dd[b], nullptr,
                      stream, mem));
     CKB_CUDA(cudaEventRecord(r.searchDone[b], stream));
@@ -148,7 +169,8 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
     CKB_CUDA(cudaEventRecord(r.downDone[b], r.down));
   }
   // the caller's stream completes after the last copy (the joiner), and the
-  // buffers are released behind it
+  // buffers are released behind it -- or the answers land behind `done`
+  if (done) CKB_CUDA(cudaEventRecord(done, r.down));
   return CUKD_OK;
 }
 
@@ -164,6 +186,21 @@ extern "C" int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *l
   if (nq > 0 && !h_queries) return CUKD_ERR_INVALID_ARGUMENT;
   return ckb::knn_pipeline(d_tree, n, layout, d_world_bounds, h_queries, nullptr, nq, params,
                            h_out_ids, h_out_d2, chunk, stream, mem);
+}
+
+extern "C" int cukd_knn_host_async(const void *d_tree, int64_t n, const cukd_layout *layout,
+                                   const void *d_world_bounds, const void *h_queries, int64_t nq,
+                                   const cukd_query_params *params, int32_t *h_out_ids,
+                                   void *h_out_d2, int64_t chunk, cudaEvent_t done,
+                                   cudaStream_t stream, const cukd_mem_resource *mem)
+{
+  if ((nq > 0 && !h_queries) || !done) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq == 0) {
+    CKB_CUDA(cudaEventRecord(done, stream));
+    return CUKD_OK;
+  }
+  return ckb::knn_pipeline(d_tree, n, layout, d_world_bounds, h_queries, nullptr, nq, params,
+                           h_out_ids, h_out_d2, chunk, stream, mem, done);
 }
 
 extern "C" int cukd_knn_to_host(const void *d_tree, int64_t n, const cukd_layout *layout,

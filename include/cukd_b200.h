@@ -274,6 +274,20 @@ CUKD_API int cukd_knn_host(const void *d_tree, int64_t n, const cukd_layout *lay
                            const cukd_query_params *params, int32_t *h_out_ids, void *h_out_d2,
                            int64_t chunk, cudaStream_t stream, const cukd_mem_resource *mem);
 
+/* cukd_knn_host that leaves `stream` free once the searches are queued: the
+ * answers are complete in h_out_ids / h_out_d2 once the caller's event
+ * `done` (created by the caller) has completed -- wait for it
+ * (cudaEventSynchronize, or cudaStreamWaitEvent before reusing those host
+ * buffers).  A caller can thus queue the next batch's build and search on
+ * the same stream while these answers are still being copied.  Up to eight
+ * device result sets per call (released on the copy stream, after the
+ * copies).  No reference counterpart. */
+CUKD_API int cukd_knn_host_async(const void *d_tree, int64_t n, const cukd_layout *layout,
+                        const void *d_world_bounds, const void *h_queries, int64_t nq,
+                        const cukd_query_params *params, int32_t *h_out_ids, void *h_out_d2,
+                        int64_t chunk, cudaEvent_t done, cudaStream_t stream,
+                        const cukd_mem_resource *mem);
+
 /* cukd_knn_host for queries already in device memory: the searches of
  * `chunk`-query slices of d_queries overlap the device->host copies of the
  * answers of the previous slices (two streams; three sets of chunk-sized

@@ -70,3 +70,43 @@ def test_knn_to_host_rejects_host_queries():
     t = torch.from_numpy(make_points(100, 3, "uniform", seed=1)).cuda()
     with pytest.raises(ValueError):
         ck.knn_to_host(t, t[:4].cpu(), 4)
+
+
+@pytest.mark.parametrize("chunk", [1000, 7777, 50000])
+def test_knn_host_async_back_to_back_batches(chunk):
+    """cukd_knn_host_async: several trees built and searched back to back on
+    one stream, each batch's answers landing behind its own event while the
+    next batch builds and searches (the host buffers of a batch reused two
+    batches later, after waiting for its event); every batch's answers equal
+    cukd_knn's."""
+    n, nq, k = 30000, 23456, 8
+    lay = ck.layout_for("float32", 3)
+    hq = torch.from_numpy(make_queries(nq, 3, "uniform", seed=4)).pin_memory()
+    slots = [{"ids": torch.empty((nq, k), dtype=torch.int32).pin_memory(),
+              "d2": torch.empty((nq, k), dtype=torch.float32).pin_memory(),
+              "done": torch.cuda.Event(), "used": False} for _ in range(2)]
+    trees, want = [], []
+    for b in range(5):
+        t = torch.from_numpy(make_points(n, 3, "uniform", seed=10 + b)).cuda()
+        wb = ck.build_tree(t, layout=lay)
+        ri, rd = ck.knn(t, hq.cuda(), k, "stack_based", layout=lay, world_bounds=wb)
+        trees.append((t, wb))
+        want.append((ri.cpu().numpy(), f32_bits(rd.cpu().numpy())))
+    torch.cuda.synchronize()
+    main = torch.cuda.current_stream()
+    for b, (t, wb) in enumerate(trees):
+        sl = slots[b % 2]
+        if sl["used"]:
+            sl["done"].synchronize()  # the batch two back has landed: check it
+            ri, rb = want[b - 2]
+            assert np.array_equal(sl["ids"].numpy(), ri)
+            assert np.array_equal(f32_bits(sl["d2"].numpy()), rb)
+        ck.knn_host(t, hq, k, "stack_based", layout=lay, world_bounds=wb, out_ids=sl["ids"],
+                    out_d2=sl["d2"], chunk=chunk, done=sl["done"])
+        sl["used"] = True
+    for b in (3, 4):
+        sl = slots[b % 2]
+        sl["done"].synchronize()
+        assert np.array_equal(sl["ids"].numpy(), want[b][0])
+        assert np.array_equal(f32_bits(sl["d2"].numpy()), want[b][1])
+    main.synchronize()
