@@ -41,7 +41,7 @@ constexpr int kMaxSets = 8;  // ... when the copies do not hold the caller's str
 struct PipeRes {
   cudaStream_t up = nullptr, down = nullptr;
   cudaEvent_t upDone[kMaxSets] = {}, searchDone[kMaxSets] = {}, downDone[kMaxSets] = {};
-  cudaEvent_t start = nullptr, join[2] = {};
+  cudaEvent_t start = nullptr, join[2] = {}, allocDone = nullptr;
   ~PipeRes()
   {
     for (int i = 0; i < kMaxSets; i++) {
@@ -50,6 +50,7 @@ struct PipeRes {
       if (downDone[i]) cudaEventDestroy(downDone[i]);
     }
     if (start) cudaEventDestroy(start);
+    if (allocDone) cudaEventDestroy(allocDone);
     for (cudaEvent_t e : join)
       if (e) cudaEventDestroy(e);
     if (up) cudaStreamDestroy(up);
@@ -122,6 +123,7 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
     CKB_CUDA(cudaEventCreateWithFlags(&r.downDone[i], cudaEventDisableTiming));
   }
   CKB_CUDA(cudaEventCreateWithFlags(&r.start, cudaEventDisableTiming));
+  CKB_CUDA(cudaEventCreateWithFlags(&r.allocDone, cudaEventDisableTiming));
   for (cudaEvent_t &e : r.join) CKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
   TempArena arena(stream, mem);
@@ -138,6 +140,12 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
   }
   // declared after the arenas: joins the side streams before they release
   JoinSideStreams joiner{r, stream, done == nullptr};
+  // result buffers taken on the copy stream are written first by the
+  // searches on the caller's stream: that stream waits for the allocations
+  if (done) {
+    CKB_CUDA(cudaEventRecord(r.allocDone, r.down));
+    CKB_CUDA(cudaStreamWaitEvent(stream, r.allocDone, 0));
+  }
   // the side streams start after the work already queued on `stream`
   CKB_CUDA(cudaEventRecord(r.start, stream));
   if (upload) CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
