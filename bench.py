@@ -67,7 +67,11 @@ def parse():
                     help="tile,block,queries_per_thread,morton for the batched section "
                          "instead of autotuning (profiling runs)")
     ap.add_argument("--e2e-chunk", type=int, default=1 << 21,
-                    help="queries per chunk of the host-buffer kNN in the e2e measurement")
+                    help="queries per chunk of the host-buffer kNN in the e2e measurements "
+                         "that run one step at a time")
+    ap.add_argument("--e2e-async-chunk", type=int, default=0,
+                    help="queries per chunk of the pipelined e2e steps (0 = the library's "
+                         "default for the asynchronous calls: the whole 10M batch)")
     ap.add_argument("--configs", default="",
                     help="comma list of c1,c2,c4,c5: measure those configurations instead "
                          "(one JSON line each, not the benchmark line)")
@@ -364,16 +368,13 @@ def run_ours(args, rank, world, local):
         h_d2 = torch.empty((nq, K), dtype=torch.float32).pin_memory()
         side = torch.cuda.Stream()
         e2e_q = torch.empty_like(d_q)
-        # two batches in flight: step i runs on stream i % 2 with its own
-        # device tree and pinned answer buffers, so its upload, build and
-        # search overlap the device->host copy of the previous step's answers
-        # (PCIe copies both ways at once; the answers, 1.28 GB, are the
-        # slowest stage)
-        # one compute stream (the current one) runs each step's build and
-        # search back to back; the next step's points go up on a side stream
-        # once its tree buffer is free; each step's answers land behind its
-        # own event (cukd_knn_host_async), so the device->host copies of one
-        # step overlap the compute of the next
+        # two batches in flight: one compute stream (the current one) runs
+        # each step's build and search back to back; the step's points and
+        # queries go up on a side stream once its slot's buffers are free;
+        # each step's answers land behind its own event
+        # (cukd_knn_to_host_async), so the device->host copy of one step's
+        # answers (1.28 GB, the slowest stage; PCIe copies both ways at once)
+        # overlaps the next step's build and search
         up_stream = torch.cuda.Stream()
         slots = []
         for j in range(2):
@@ -381,8 +382,9 @@ def run_ours(args, rank, world, local):
                           "wb": wb if j == 0 else torch.empty_like(wb),
                           "ids": h_ids if j == 0 else torch.empty_like(h_ids).pin_memory(),
                           "d2": h_d2 if j == 0 else torch.empty_like(h_d2).pin_memory(),
+                          "q": torch.empty((nq, 3), dtype=torch.float32, device=dev),
                           "done": torch.cuda.Event(), "free": torch.cuda.Event(),
-                          "up": torch.cuda.Event(), "used": False})
+                          "up": torch.cuda.Event(), "upq": torch.cuda.Event(), "used": False})
         step_no = [0]
 
         def pipelined_step():
@@ -393,31 +395,41 @@ def run_ours(args, rank, world, local):
                 up_stream.wait_event(sl["free"])  # the search two steps back has run
             with torch.cuda.stream(up_stream):
                 sl["pts"].copy_(h_pts, non_blocking=True)
-            sl["up"].record(up_stream)
+                sl["up"].record(up_stream)
+                sl["q"].copy_(h_q, non_blocking=True)
+                sl["upq"].record(up_stream)
             main.wait_event(sl["up"])
+            ck.build_tree(sl["pts"], layout=lay, world_bounds=sl["wb"])
             if sl["used"]:
                 main.wait_event(sl["done"])  # its host buffers: that step's answers landed
-            ck.build_tree(sl["pts"], layout=lay, world_bounds=sl["wb"])
-            ck.knn_host(sl["pts"], h_q, K, "stack_based", layout=lay, world_bounds=sl["wb"],
-                        out_ids=sl["ids"], out_d2=sl["d2"], chunk=args.e2e_chunk,
-                        done=sl["done"])
+            main.wait_event(sl["upq"])
+            sl["done"] = torch.cuda.Event(enable_timing=True)  # one per step: timed below
+            ck.knn_to_host(sl["pts"], sl["q"], K, "stack_based", layout=lay,
+                           world_bounds=sl["wb"], out_ids=sl["ids"], out_d2=sl["d2"],
+                           chunk=args.e2e_async_chunk, done=sl["done"])
             sl["free"].record(main)
             sl["used"] = True
+            return sl["done"]
 
         def timed_pipelined():
-            for _ in range(2):
-                pipelined_step()
+            for _ in range(max(2, args.warmup)):
+                warm_done = pipelined_step()
             barrier()
             main = torch.cuda.current_stream()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(main)
             for _ in range(args.steps):
-                pipelined_step()
+                last_done = pipelined_step()
             for sl in slots:
                 main.wait_event(sl["done"])
             b.record(main)
             barrier()
-            return max_over_ranks(a.elapsed_time(b), pg, dev) / args.steps
+            # the window from the queueing point also holds the rest of the
+            # last warm-up step's answer copies; the steady-state figure runs
+            # from those answers landing to the last timed step's
+            steady = warm_done.elapsed_time(last_done)
+            return (max_over_ranks(a.elapsed_time(b), pg, dev) / args.steps,
+                    max_over_ranks(steady, pg, dev) / args.steps)
 
         def e2e_step():
             # points up, build, then cukd_knn_host: query chunks copied up,
@@ -451,10 +463,11 @@ def run_ours(args, rank, world, local):
             barrier()
             return max_over_ranks(a.elapsed_time(b), pg, dev) / args.steps
 
-        et = timed_pipelined()
+        et, steady_ms = timed_pipelined()
         st_ms = timed(e2e_step)
         dt = timed(device_queries_step)
         slots[1]["pts"] = slots[1]["ids"] = slots[1]["d2"] = None
+        slots[0]["q"] = slots[1]["q"] = None
 
         # the PCIe copies alone (one whole-array copy each way, pinned host
         # memory): the floor under any e2e step that moves these bytes
@@ -480,11 +493,20 @@ def run_ours(args, rank, world, local):
                "d2h_bytes_per_step": int(h_ids.numel() * 4 + h_d2.numel() * 4),
                "ms_per_step": round(et, 3),
                "pcie_copies_alone_ms": {"h2d": round(up_ms, 3), "d2h": round(down_ms, 3)},
-               "api": (f"cukd_build_tree + cukd_knn_host_async (pinned host queries and "
-                       f"results, {args.e2e_chunk}-query chunks on overlapping copy / search "
-                       "streams) on one stream, each step's answers landing behind its own "
-                       "event while the next step builds and searches; the next step's points "
-                       "uploaded on a side stream; two device trees and answer buffers"),
+               "api": ("cukd_build_tree + cukd_knn_to_host_async (pinned host results, "
+                       + (f"{args.e2e_async_chunk}-query chunks" if args.e2e_async_chunk > 0
+                          else "the batch searched in one slice") +
+                       ") on one stream, each step's answers copied down behind its "
+                       "own event while the next step builds and searches; each step's "
+                       "points and queries copied up from pinned host memory on a side "
+                       "stream during the previous step; two device trees, query and answer "
+                       "buffers"),
+               "steady_state": {
+                   "value": round(whole_job_rate(nq, world, steady_ms), 1),
+                   "ms_per_step": round(steady_ms, 3),
+                   "window": "the same steps, from the last warm-up step's answers landing in "
+                             "host memory to the last timed step's (ms_per_step above also "
+                             "holds the rest of the warm-up step's answer copies)"},
                "one_step_at_a_time": {
                    "value": round(whole_job_rate(nq, world, st_ms), 1),
                    "ms_per_step": round(st_ms, 3),

@@ -356,6 +356,12 @@ def knn(tree, queries, k, method="stack_based", layout=None, world_bounds=None, 
     return (ids, d2, mx) if with_max else (ids, d2)
 
 
+def _init_event(ev, stream):
+    """torch creates a CUDA event at its first record: record it once."""
+    if not ev.cuda_event:
+        ev.record(stream if isinstance(stream, torch.cuda.Stream) else torch.cuda.current_stream())
+
+
 def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
              cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, out_ids=None, out_d2=None,
              chunk=0, stream=None, done=None):
@@ -379,9 +385,7 @@ def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=N
     d2 = out_d2 if out_d2 is not None else torch.empty((nq, k), dtype=dt, pin_memory=pin)
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
     if done is not None:
-        if not done.cuda_event:  # created lazily by torch: record once to create it
-            done.record(stream if isinstance(stream, torch.cuda.Stream)
-                        else torch.cuda.current_stream())
+        _init_event(done, stream)
         L = lib()
         L.cukd_knn_host_async.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Layout), C.c_void_p,
                                           C.c_void_p, C.c_int64, C.POINTER(QueryParams),
@@ -400,12 +404,14 @@ def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=N
 
 def knn_to_host(tree, queries, k, method="stack_based", layout=None, world_bounds=None, n=None,
                 cutoff=math.inf, cutoff_d2=INT64_MAX, morton=True, out_ids=None, out_d2=None,
-                chunk=0, stream=None):
+                chunk=0, stream=None, done=None):
     """knn() of device-resident queries with the answers written to host
     memory (pinned CPU tensors by default), searches of query slices
     overlapping the copies of earlier answers.  Returns (ids, d2) CPU
     tensors, complete once ``stream`` (default: the current stream) is
-    synchronised."""
+    synchronised -- or, with ``done`` (a torch.cuda.Event), once that event
+    has completed, the stream being free as soon as the searches are queued
+    (cukd_knn_to_host_async)."""
     layout = layout or infer_layout(tree)
     if n is None:
         n = _num_records(tree, layout)
@@ -420,6 +426,18 @@ def knn_to_host(tree, queries, k, method="stack_based", layout=None, world_bound
     if ids.is_cuda or d2.is_cuda:
         raise ValueError("out_ids / out_d2 must be host memory")
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
+    if done is not None:
+        _init_event(done, stream)
+        L = lib()
+        L.cukd_knn_to_host_async.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Layout),
+                                             C.c_void_p, C.c_void_p, C.c_int64,
+                                             C.POINTER(QueryParams), C.c_void_p, C.c_void_p,
+                                             C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        _check(L.cukd_knn_to_host_async(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                                        _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2),
+                                        int(chunk), C.c_void_p(done.cuda_event),
+                                        _stream(stream), None), "cukd_knn_to_host_async")
+        return ids, d2
     _check(lib().cukd_knn_to_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
                                   _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk),
                                   _stream(stream), None), "cukd_knn_to_host")

@@ -59,8 +59,10 @@ void keep_default_pool_memory();
 struct TempArena {
   cudaStream_t stream;
   const cukd_mem_resource *mem;
+  cudaMemPool_t pool;  // without a caller's resource: this pool, else the device's default
   std::vector<void *> ptrs;
-  TempArena(cudaStream_t s, const cukd_mem_resource *m) : stream(s), mem(m)
+  TempArena(cudaStream_t s, const cukd_mem_resource *m, cudaMemPool_t p = nullptr)
+      : stream(s), mem(m), pool(p)
   {
     if (!mem || !mem->alloc) keep_default_pool_memory();
   }
@@ -80,7 +82,8 @@ struct TempArena {
       if (mem->alloc(mem->ctx, &p, bytes + 16, stream) != 0 || !p) return CUKD_ERR_OUT_OF_MEMORY;
       use = reinterpret_cast<void *>((reinterpret_cast<uintptr_t>(p) + 15u) & ~uintptr_t(15));
     } else {
-      cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+      cudaError_t e =
+          pool ? cudaMallocFromPoolAsync(&p, bytes, pool, stream) : cudaMallocAsync(&p, bytes, stream);
       if (e != cudaSuccess) {
         cudaGetLastError();
         return e == cudaErrorMemoryAllocation ? CUKD_ERR_OUT_OF_MEMORY : CUKD_ERR_CUDA;

@@ -15,15 +15,18 @@
 // whose queries and answers live in host memory (the reference's samples
 // copy whole arrays with cudaMemcpy around one query launch,
 // sample.cu:121-160); results are those of cukd_knn.
-//   cukd_knn_host_async  cukd_knn_host that leaves the caller's stream free
+//   cukd_knn_host_async / cukd_knn_to_host_async
+//                     cukd_knn_host / cukd_knn_to_host that leave the caller's stream free
 //                     once the searches are queued: the answers land behind
 //                     the caller's event `done` (the result buffers, up to
 //                     eight sets, are released on the copy stream), so a
 //                     caller can queue the next tree's build and search on
 //                     the same stream while these answers are still being
 //                     copied -- the compute and the device->host copies of
-//                     consecutive batches then overlap.
+//                     consecutive batches then overlap, and by default a
+//                     batch of up to 2^24 queries is searched in one slice.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -57,6 +60,46 @@ struct PipeRes {
     if (down) cudaStreamDestroy(down);
   }
 };
+
+// The result buffers of the asynchronous calls (no caller's resource) come
+// from a pool of their own that never makes an allocation wait for a
+// release queued on another stream: the device's default pool may hand a
+// call the buffers that the previous call releases behind its device->host
+// copies, and the call's searches would then wait for those copies.  This
+// pool reuses memory whose release has run, or whose release the copy
+// stream already follows (a caller that waited for an earlier call's `done`
+// before this call), else it grows; it keeps what it holds for the next
+// call, like the default pool does for this library's other temporaries.
+cudaMemPool_t result_pool()
+{
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;  // the default pool then
+    }
+    uint64_t keep = UINT64_MAX;
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    cudaGetLastError();
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
 
 // On every exit, success or error: the caller's stream waits for all work
 // queued on the side streams (only the upload stream when the answers land
@@ -106,7 +149,11 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
   const int k = params->k;
   const int64_t qBytes = int64_t(L.D) * 4;
   const int64_t d2Bytes = L.scalar == CUKD_FLOAT32 ? 4 : 8;
-  if (chunk <= 0) chunk = int64_t(1) << 20;
+  // the asynchronous calls overlap one call's copies with the next call's
+  // build and search, so slicing a batch only adds per-search cost (10M
+  // queries, k = 16, back to back: 23.8 ms a batch in one slice, 24.6 in
+  // 5M-query slices, 26.8 in 2^21): one slice up to 2^24 queries
+  if (chunk <= 0) chunk = done ? int64_t(1) << 24 : int64_t(1) << 20;
   chunk = std::min(chunk, nq);
 
   PipeRes r;
@@ -126,10 +173,18 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
   CKB_CUDA(cudaEventCreateWithFlags(&r.allocDone, cudaEventDisableTiming));
   for (cudaEvent_t &e : r.join) CKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
+  // the side streams start after the work already queued on `stream` --
+  // also the result buffers' allocations on the copy stream: memory that an
+  // earlier call released before its `done`, which the caller's stream has
+  // waited for, is then reused without waiting for anything else
+  CKB_CUDA(cudaEventRecord(r.start, stream));
+  if (upload) CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
+  CKB_CUDA(cudaStreamWaitEvent(r.down, r.start, 0));
   TempArena arena(stream, mem);
   // the result buffers: released on the copy stream when the answers land
   // behind `done` (after the copies), else on the caller's stream
-  TempArena downArena(done ? r.down : stream, mem);
+  TempArena downArena(done ? r.down : stream, mem,
+                      done && !(mem && mem->alloc) ? result_pool() : nullptr);
   uint8_t *dq[kMaxSets] = {};
   int32_t *di[kMaxSets];
   uint8_t *dd[kMaxSets] = {};
@@ -146,10 +201,6 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
     CKB_CUDA(cudaEventRecord(r.allocDone, r.down));
     CKB_CUDA(cudaStreamWaitEvent(stream, r.allocDone, 0));
   }
-  // the side streams start after the work already queued on `stream`
-  CKB_CUDA(cudaEventRecord(r.start, stream));
-  if (upload) CKB_CUDA(cudaStreamWaitEvent(r.up, r.start, 0));
-  CKB_CUDA(cudaStreamWaitEvent(r.down, r.start, 0));
   for (int64_t c = 0; c < chunks; c++) {
     const int b = int(c % sets);
     const int64_t q0 = c * chunk, m = std::min(chunk, nq - q0);
@@ -178,7 +229,12 @@ int knn_pipeline(const void *d_tree, int64_t n, const cukd_layout *layout,
   }
   // the caller's stream completes after the last copy (the joiner), and the
   // buffers are released behind it -- or the answers land behind `done`
-  if (done) CKB_CUDA(cudaEventRecord(done, r.down));
+  // (every search has its copies queued behind it on the copy stream, so
+  // the result buffers are released there before `done`)
+  if (done) {
+    downArena.release_all();
+    CKB_CUDA(cudaEventRecord(done, r.down));
+  }
   return CUKD_OK;
 }
 
@@ -220,4 +276,20 @@ extern "C" int cukd_knn_to_host(const void *d_tree, int64_t n, const cukd_layout
   if (nq > 0 && !d_queries) return CUKD_ERR_INVALID_ARGUMENT;
   return ckb::knn_pipeline(d_tree, n, layout, d_world_bounds, nullptr, d_queries, nq, params,
                            h_out_ids, h_out_d2, chunk, stream, mem);
+}
+
+extern "C" int cukd_knn_to_host_async(const void *d_tree, int64_t n, const cukd_layout *layout,
+                                      const void *d_world_bounds, const void *d_queries,
+                                      int64_t nq, const cukd_query_params *params,
+                                      int32_t *h_out_ids, void *h_out_d2, int64_t chunk,
+                                      cudaEvent_t done, cudaStream_t stream,
+                                      const cukd_mem_resource *mem)
+{
+  if ((nq > 0 && !d_queries) || !done) return CUKD_ERR_INVALID_ARGUMENT;
+  if (nq == 0) {
+    CKB_CUDA(cudaEventRecord(done, stream));
+    return CUKD_OK;
+  }
+  return ckb::knn_pipeline(d_tree, n, layout, d_world_bounds, nullptr, d_queries, nq, params,
+                           h_out_ids, h_out_d2, chunk, stream, mem, done);
 }

@@ -110,3 +110,36 @@ def test_knn_host_async_back_to_back_batches(chunk):
         assert np.array_equal(sl["ids"].numpy(), want[b][0])
         assert np.array_equal(f32_bits(sl["d2"].numpy()), want[b][1])
     main.synchronize()
+
+
+def test_knn_to_host_async_back_to_back_batches():
+    """cukd_knn_to_host_async: device-resident queries, several trees
+    searched back to back on one stream with each batch's answers behind its
+    own event; every batch's answers equal cukd_knn's."""
+    n, nq, k = 30000, 23456, 16
+    lay = ck.layout_for("float32", 3)
+    dq = torch.from_numpy(make_queries(nq, 3, "uniform", seed=6)).cuda()
+    slots = [{"ids": torch.empty((nq, k), dtype=torch.int32).pin_memory(),
+              "d2": torch.empty((nq, k), dtype=torch.float32).pin_memory(),
+              "done": torch.cuda.Event(), "used": False} for _ in range(2)]
+    trees, want = [], []
+    for b in range(5):
+        t = torch.from_numpy(make_points(n, 3, "gmm", seed=20 + b)).cuda()
+        wb = ck.build_tree(t, layout=lay)
+        ri, rd = ck.knn(t, dq, k, "stack_based", layout=lay, world_bounds=wb)
+        trees.append((t, wb))
+        want.append((ri.cpu().numpy(), f32_bits(rd.cpu().numpy())))
+    for b, (t, wb) in enumerate(trees):
+        sl = slots[b % 2]
+        if sl["used"]:
+            sl["done"].synchronize()
+            assert np.array_equal(sl["ids"].numpy(), want[b - 2][0])
+            assert np.array_equal(f32_bits(sl["d2"].numpy()), want[b - 2][1])
+        ck.knn_to_host(t, dq, k, "stack_based", layout=lay, world_bounds=wb, out_ids=sl["ids"],
+                       out_d2=sl["d2"], chunk=5000, done=sl["done"])
+        sl["used"] = True
+    for b in (3, 4):
+        sl = slots[b % 2]
+        sl["done"].synchronize()
+        assert np.array_equal(sl["ids"].numpy(), want[b][0])
+        assert np.array_equal(f32_bits(sl["d2"].numpy()), want[b][1])
