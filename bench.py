@@ -413,23 +413,24 @@ def run_ours(args, rank, world, local):
 
         def timed_pipelined():
             for _ in range(max(2, args.warmup)):
-                warm_done = pipelined_step()
+                pipelined_step()
             barrier()
             main = torch.cuda.current_stream()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(main)
-            for _ in range(args.steps):
-                last_done = pipelined_step()
+            dones = [pipelined_step() for _ in range(args.steps)]
             for sl in slots:
                 main.wait_event(sl["done"])
             b.record(main)
             barrier()
-            # the window from the queueing point also holds the rest of the
-            # last warm-up step's answer copies; the steady-state figure runs
-            # from those answers landing to the last timed step's
-            steady = warm_done.elapsed_time(last_done)
+            # the window opens on a drained device (the barrier synchronises),
+            # so the first step's upload, build, search and answer copies run
+            # back to back; the steady-state figure is the interval between
+            # consecutive steps' answers landing, over the timed steps
+            steady = (dones[0].elapsed_time(dones[-1]) / (args.steps - 1) if args.steps > 1
+                      else a.elapsed_time(b))
             return (max_over_ranks(a.elapsed_time(b), pg, dev) / args.steps,
-                    max_over_ranks(steady, pg, dev) / args.steps)
+                    max_over_ranks(steady, pg, dev))
 
         def e2e_step():
             # points up, build, then cukd_knn_host: query chunks copied up,
@@ -504,9 +505,11 @@ def run_ours(args, rank, world, local):
                "steady_state": {
                    "value": round(whole_job_rate(nq, world, steady_ms), 1),
                    "ms_per_step": round(steady_ms, 3),
-                   "window": "the same steps, from the last warm-up step's answers landing in "
-                             "host memory to the last timed step's (ms_per_step above also "
-                             "holds the rest of the warm-up step's answer copies)"},
+                   "window": "the same steps: the interval between consecutive steps' answers "
+                             "landing in host memory, from the first timed step's to the last's "
+                             "(ms_per_step above opens on a drained device, so it also holds one "
+                             "pipeline fill: the first step's upload, build, search and copies "
+                             "back to back)"},
                "one_step_at_a_time": {
                    "value": round(whole_job_rate(nq, world, st_ms), 1),
                    "ms_per_step": round(st_ms, 3),
