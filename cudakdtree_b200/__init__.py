@@ -210,6 +210,10 @@ def lib():
                                     C.POINTER(QueryParams), P, P, I64, P, P]
         L.cukd_knn_to_host.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
                                        C.POINTER(QueryParams), P, P, I64, P, P]
+        L.cukd_knn_host_async.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
+                                          C.POINTER(QueryParams), P, P, I64, P, P, P]
+        L.cukd_knn_to_host_async.argtypes = [P, I64, C.POINTER(Layout), P, P, I64,
+                                             C.POINTER(QueryParams), P, P, I64, P, P, P]
         L.cukd_knn_accumulate.argtypes = [P, I64, C.POINTER(Layout), P, I64, P, I64, P, C.c_int,
                                           C.c_float, C.c_int, P, P]
         L.cukd_knn_lists_extract.argtypes = [P, I64, C.c_int, P, P, P, P]
@@ -386,15 +390,10 @@ def knn_host(tree, queries, k, method="stack_based", layout=None, world_bounds=N
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
     if done is not None:
         _init_event(done, stream)
-        L = lib()
-        L.cukd_knn_host_async.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Layout), C.c_void_p,
-                                          C.c_void_p, C.c_int64, C.POINTER(QueryParams),
-                                          C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
-                                          C.c_void_p, C.c_void_p]
-        _check(L.cukd_knn_host_async(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
-                                     _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2),
-                                     int(chunk), C.c_void_p(done.cuda_event), _stream(stream),
-                                     None), "cukd_knn_host_async")
+        _check(lib().cukd_knn_host_async(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
+                                         _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2),
+                                         int(chunk), C.c_void_p(done.cuda_event),
+                                         _stream(stream), None), "cukd_knn_host_async")
         return ids, d2
     _check(lib().cukd_knn_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds), _ptr(queries),
                                nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk), _stream(stream),
@@ -428,15 +427,11 @@ def knn_to_host(tree, queries, k, method="stack_based", layout=None, world_bound
     p = _params(method, k, cutoff, 0.0, cutoff_d2, morton)
     if done is not None:
         _init_event(done, stream)
-        L = lib()
-        L.cukd_knn_to_host_async.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Layout),
-                                             C.c_void_p, C.c_void_p, C.c_int64,
-                                             C.POINTER(QueryParams), C.c_void_p, C.c_void_p,
-                                             C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
-        _check(L.cukd_knn_to_host_async(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
-                                        _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2),
-                                        int(chunk), C.c_void_p(done.cuda_event),
-                                        _stream(stream), None), "cukd_knn_to_host_async")
+        _check(lib().cukd_knn_to_host_async(_ptr(tree), n, C.byref(layout),
+                                            _ptr(world_bounds), _ptr(queries), nq, C.byref(p),
+                                            _ptr(ids), _ptr(d2), int(chunk),
+                                            C.c_void_p(done.cuda_event), _stream(stream),
+                                            None), "cukd_knn_to_host_async")
         return ids, d2
     _check(lib().cukd_knn_to_host(_ptr(tree), n, C.byref(layout), _ptr(world_bounds),
                                   _ptr(queries), nq, C.byref(p), _ptr(ids), _ptr(d2), int(chunk),

@@ -56,3 +56,37 @@ def test_invalid_layouts_are_rejected_before_any_device_work():
     # empty input is a no-op even without a device (builder_thrust.h:441)
     assert L.cukd_build_tree(None, 0, C.byref(ck.layout_for("float32", 3)), None, 0, None,
                              None) == 0
+
+
+def test_host_buffer_knn_refuses_bad_arguments_before_any_device_work():
+    """The host-buffer kNN entry points check their arguments before they
+    create a stream or touch memory: no queries, no answer buffer, k out of
+    range, a bad layout or (asynchronous forms) no completion event give
+    CUKD_ERR_INVALID_ARGUMENT; an empty batch is a no-op."""
+    import ctypes as C
+    import cudakdtree_b200 as ck
+    L = ck.lib()
+    lay = ck.layout_for("float32", 3)
+    p = ck.QueryParams()
+    L.cukd_query_params_init(p)
+    p.k = 16
+    fake = C.c_void_p(4096)  # never dereferenced: every call below fails first
+    host = L.cukd_knn_host, L.cukd_knn_to_host
+    for f in host:
+        assert f(fake, 10, C.byref(lay), None, None, 5, C.byref(p), fake, fake, 0, None, None) == 1
+        assert f(fake, 10, C.byref(lay), None, fake, 5, C.byref(p), None, fake, 0, None, None) == 1
+        assert f(fake, 10, C.byref(ck.layout_for("float32", 9)), None, fake, 5, C.byref(p), fake,
+                 fake, 0, None, None) == 1
+        assert f(fake, 10, C.byref(lay), None, fake, 0, C.byref(p), fake, fake, 0, None, None) == 0
+    for f in (L.cukd_knn_host_async, L.cukd_knn_to_host_async):
+        assert f(fake, 10, C.byref(lay), None, fake, 5, C.byref(p), fake, fake, 0, None, None,
+                 None) == 1  # no event
+        assert f(fake, 10, C.byref(lay), None, None, 5, C.byref(p), fake, fake, 0, fake, None,
+                 None) == 1  # no queries
+    bad_k = ck.QueryParams()
+    L.cukd_query_params_init(bad_k)
+    for k in (0, 1025):
+        bad_k.k = k
+        for f in host:
+            assert f(fake, 10, C.byref(lay), None, fake, 5, C.byref(bad_k), fake, fake, 0, None,
+                     None) == 1
