@@ -1,6 +1,6 @@
 // Stable LSD radix sort, 8 bits per pass: per-tile digit histograms, one
 // exclusive scan over (digit, tile), and a scatter that ranks equal digits
-// in index order with warp match/ballot so every pass is stable.
+// in index order with warp match so every pass is stable.
 #include <algorithm>
 
 #include "sort.cuh"
@@ -75,61 +75,117 @@ __global__ void __launch_bounds__(kThreads) column_scan_kernel(uint32_t *counts,
   if (threadIdx.x == 0) digitTotals[blockIdx.x] = carry;
 }
 
-__global__ void __launch_bounds__(kThreads) scatter_kernel(
+// One tile of kTileItems keys per CTA.  Warp w owns the tile's positions
+// [w * 512, (w + 1) * 512), lane l its items w * 512 + 32 j + l (j < 16), so
+// ranking the items of a digit in (warp, j, lane) order is index order: the
+// pass is stable.  Each item's rank among its warp's items of that digit
+// comes from match_any over the rounds; digit-major offsets over the warps
+// and over the digits place it in the tile; the tile is staged in shared
+// memory in digit order and written out in that order, so the writes of a
+// digit's run from this tile are consecutive addresses.  (The earlier form
+// ranked 256 items at a time with three barriers each and wrote straight
+// to global memory: 180 us a pass over 10M keys in a cold ncu replay.)
+__global__ void __launch_bounds__(kThreads, 3) scatter_kernel(
     const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, int64_t n, int shift,
     int numTiles, const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ digitTotals,
     uint32_t *__restrict__ keysOut, uint32_t *__restrict__ valsOut)
 {
   constexpr int W = kThreads / 32;
-  __shared__ uint32_t running[256];
-  __shared__ uint32_t wcnt[W][256];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  {
-    // exclusive prefix of the 256 digit totals (computed by every CTA)
-    const uint32_t t = digitTotals[threadIdx.x];
-    uint32_t incl = t;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += u;
-    }
-    if (lane == 31) wcnt[0][wid] = incl;
-    __syncthreads();
-    uint32_t wbase = 0;
-    for (int w = 0; w < wid; w++) wbase += wcnt[0][w];
-    running[threadIdx.x] = offsets[int64_t(threadIdx.x) * numTiles + blockIdx.x] + wbase + incl - t;
-    __syncthreads();
-  }
-  for (int w = 0; w < W; w++) wcnt[w][threadIdx.x] = 0;
-  __syncthreads();
+  constexpr int kWarpItems = kTileItems / W;
+  static_assert(kWarpItems == 32 * kItems, "a warp's items: kItems rounds of 32");
+  static_assert(kThreads == 256, "a thread per digit");
+  __shared__ uint32_t sk[kTileItems], sv[kTileItems];
+  __shared__ uint16_t wh[W][256];     // per warp and digit: count, then exclusive offset
+  __shared__ uint32_t tileStart[256];  // a digit's first position in the tile
+  __shared__ uint32_t outBase[256];    // a digit's first output position from this tile
+  __shared__ uint32_t red[2][W];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int64_t base = int64_t(blockIdx.x) * kTileItems;
-  const uint32_t ltMask = (1u << lane) - 1u;
+  const int64_t wbase = base + int64_t(wid) * kWarpItems;
+  for (int i = tid; i < W * 256; i += kThreads) (&wh[0][0])[i] = 0;
+  // this warp's items in the tile: positions below lim are in the input
+  const int64_t rem = n - wbase;
+  const int lim = rem <= 0 ? 0 : (rem < kWarpItems ? int(rem) : kWarpItems);
+  const uint32_t *kw = keys + wbase, *vw = vals + wbase;
+  uint32_t k[kItems], v[kItems];
+#pragma unroll
   for (int j = 0; j < kItems; j++) {
-    const int64_t i = base + j * kThreads + threadIdx.x;
-    const bool valid = i < n;
-    const uint32_t k = valid ? keys[i] : 0u;
-    const uint32_t v = valid ? vals[i] : 0u;
-    const uint32_t digit = valid ? ((k >> shift) & 255u) : 256u + lane;
-    const uint32_t peers = __match_any_sync(0xffffffffu, digit);
-    const uint32_t rank = __popc(peers & ltMask);
-    if (valid && rank == 0) wcnt[wid][digit] = __popc(peers);
-    __syncthreads();
-    if (valid) {
-      uint32_t pre = 0;
-      for (int w = 0; w < wid; w++) pre += wcnt[w][digit];
-      const uint32_t pos = running[digit] + pre + rank;
-      keysOut[pos] = k;
-      valsOut[pos] = v;
+    const int i = j * 32 + lane;
+    k[j] = i < lim ? kw[i] : 0u;
+    v[j] = i < lim ? vw[i] : 0u;
+  }
+  __syncthreads();
+  const uint32_t ltMask = (1u << lane) - 1u;
+  uint32_t r[kItems / 2];  // ranks (< 512), two per word
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const bool valid = j * 32 + lane < lim;
+    const uint32_t d = valid ? (k[j] >> shift) & 255u : 256u + lane;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t below = __popc(peers & ltMask);
+    const uint32_t cnt = valid ? uint32_t(wh[wid][d]) : 0u;
+    __syncwarp();  // every lane has read the count before its leader adds
+    if (valid && below == 0) wh[wid][d] = uint16_t(cnt + __popc(peers));
+    __syncwarp();
+    if (j & 1)
+      r[j >> 1] |= (cnt + below) << 16;
+    else
+      r[j >> 1] = cnt + below;
+  }
+  __syncthreads();
+  {
+    // thread tid owns digit tid: the warps' exclusive offsets (digit-major),
+    // then exclusive scans over the digits of the tile's counts and of the
+    // digit totals of the whole pass
+    const int d = tid;
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      const uint32_t c = wh[w][d];
+      wh[w][d] = uint16_t(run);
+      run += c;
     }
-    __syncthreads();
-    {
-      uint32_t tot = 0;
-      for (int w = 0; w < W; w++) {
-        tot += wcnt[w][threadIdx.x];
-        wcnt[w][threadIdx.x] = 0;
+    const uint32_t tot = digitTotals[d];
+    uint32_t a = run, b = tot;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t ta = __shfl_up_sync(0xffffffffu, a, o);
+      const uint32_t tb = __shfl_up_sync(0xffffffffu, b, o);
+      if (lane >= o) {
+        a += ta;
+        b += tb;
       }
-      running[threadIdx.x] += tot;
+    }
+    if (lane == 31) {
+      red[0][wid] = a;
+      red[1][wid] = b;
     }
     __syncthreads();
+    uint32_t pa = 0, pb = 0;
+    for (int w = 0; w < wid; w++) {
+      pa += red[0][w];
+      pb += red[1][w];
+    }
+    tileStart[d] = pa + a - run;
+    outBase[d] = offsets[int64_t(d) * numTiles + blockIdx.x] + pb + b - tot;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    if (j * 32 + lane < lim) {
+      const uint32_t d = (k[j] >> shift) & 255u;
+      const uint32_t p = tileStart[d] + wh[wid][d] + ((r[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+      sk[p] = k[j];
+      sv[p] = v[j];
+    }
+  }
+  __syncthreads();
+  const int m = n - base < kTileItems ? int(n - base) : kTileItems;
+  for (int p = tid; p < m; p += kThreads) {
+    const uint32_t key = sk[p];
+    const uint32_t d = (key >> shift) & 255u;
+    const uint32_t g = outBase[d] + uint32_t(p) - tileStart[d];
+    keysOut[g] = key;
+    valsOut[g] = sv[p];
   }
 }
 

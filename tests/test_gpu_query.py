@@ -185,6 +185,36 @@ def test_morton_order_is_a_permutation():
     assert np.array_equal(np.sort(perm), np.arange(len(q)))
 
 
+def _morton_codes(cells, D):
+    bits = 30 // D
+    code = np.zeros(len(cells), np.uint64)
+    for d in range(D):
+        c = cells[:, d].astype(np.uint64)
+        for b in range(bits):
+            code |= ((c >> np.uint64(b)) & np.uint64(1)) << np.uint64(b * D + (D - 1 - d))
+    return code
+
+
+@pytest.mark.parametrize("D", [2, 3, 4])
+@pytest.mark.parametrize("n", [1, 4095, 4097, 1_000_003])
+def test_morton_order_is_the_stable_sort_of_the_codes(D, n):
+    """With bounds [0, 1] the grid scale is a power of two, so points at
+    (cell + 1/2) / 2^bits fall in known cells: the permutation must be
+    numpy's stable argsort of their Morton codes (sorted, equal codes in
+    input order) -- half the points in a few cells, so equal codes abound,
+    across many sort tiles and a partial last one."""
+    bits = 30 // D
+    rng = np.random.default_rng(n + D)
+    cells = rng.integers(0, 1 << bits, size=(n, D))
+    few = rng.random(n) < 0.5
+    cells[few] = rng.integers(0, 4, size=(int(few.sum()), D))
+    pts = ((cells + 0.5) / float(1 << bits)).astype(np.float32)
+    bounds = torch.tensor([[0.0] * D, [1.0] * D], dtype=torch.float32, device="cuda")
+    perm = ck.morton_order(torch.from_numpy(pts).cuda(), bounds=bounds).cpu().numpy()
+    want = np.argsort(_morton_codes(cells, D), kind="stable")
+    assert np.array_equal(perm, want.astype(np.int32))
+
+
 @pytest.mark.parametrize("kind", ["uniform", "tie", "gmm"])
 @pytest.mark.parametrize("explicit", [False, True])
 def test_tree_path_order_same_answers(kind, explicit):
