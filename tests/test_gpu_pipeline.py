@@ -112,10 +112,12 @@ def test_knn_host_async_back_to_back_batches(chunk):
     main.synchronize()
 
 
-def test_knn_to_host_async_back_to_back_batches():
+@pytest.mark.parametrize("chunk", [0, 2000, 5000])
+def test_knn_to_host_async_back_to_back_batches(chunk):
     """cukd_knn_to_host_async: device-resident queries, several trees
     searched back to back on one stream with each batch's answers behind its
-    own event; every batch's answers equal cukd_knn's."""
+    own event; every batch's answers equal cukd_knn's -- in one slice (the
+    default), in 12 slices (the eight result sets reused) and in 5."""
     n, nq, k = 30000, 23456, 16
     lay = ck.layout_for("float32", 3)
     dq = torch.from_numpy(make_queries(nq, 3, "uniform", seed=6)).cuda()
@@ -136,10 +138,57 @@ def test_knn_to_host_async_back_to_back_batches():
             assert np.array_equal(sl["ids"].numpy(), want[b - 2][0])
             assert np.array_equal(f32_bits(sl["d2"].numpy()), want[b - 2][1])
         ck.knn_to_host(t, dq, k, "stack_based", layout=lay, world_bounds=wb, out_ids=sl["ids"],
-                       out_d2=sl["d2"], chunk=5000, done=sl["done"])
+                       out_d2=sl["d2"], chunk=chunk, done=sl["done"])
         sl["used"] = True
     for b in (3, 4):
         sl = slots[b % 2]
         sl["done"].synchronize()
         assert np.array_equal(sl["ids"].numpy(), want[b][0])
         assert np.array_equal(f32_bits(sl["d2"].numpy()), want[b][1])
+
+
+def test_knn_to_host_async_with_a_caller_memory_resource():
+    """With the caller's memory resource the result buffers come from it
+    (taken and released on the copy stream) instead of the library's pool:
+    once `done` has completed every block is back, and the answers equal
+    cukd_knn's."""
+    import ctypes as C
+    n, nq, k = 30000, 23456, 16
+    lay = ck.layout_for("float32", 3)
+    t = torch.from_numpy(make_points(n, 3, "gmm", seed=8)).cuda()
+    wb = ck.build_tree(t, layout=lay)
+    dq = torch.from_numpy(make_queries(nq, 3, "gmm", seed=9)).cuda()
+    ri, rd = ck.knn(t, dq, k, "stack_based", layout=lay, world_bounds=wb)
+    blocks, taken = {}, [0]
+
+    def alloc(ctx, out, nbytes, stream):
+        buf = torch.empty(int(nbytes), dtype=torch.uint8, device="cuda")
+        blocks[buf.data_ptr()] = buf
+        taken[0] += 1
+        out[0] = buf.data_ptr()
+        return 0
+
+    def release(ctx, ptr, stream):
+        blocks.pop(ptr)
+        return 0
+
+    a_fn, r_fn = ck._ALLOC_FN(alloc), ck._RELEASE_FN(release)
+    mr = ck.MemResource(None, C.cast(a_fn, C.c_void_p), C.cast(r_fn, C.c_void_p))
+    ids = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    d2 = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    p = ck.QueryParams()
+    ck.lib().cukd_query_params_init(p)
+    p.k = k
+    done = torch.cuda.Event()
+    ck._init_event(done, torch.cuda.current_stream())
+    rc = ck.lib().cukd_knn_to_host_async(t.data_ptr(), n, C.byref(lay), wb.data_ptr(),
+                                         dq.data_ptr(), nq, C.byref(p), ids.data_ptr(),
+                                         d2.data_ptr(), 4000, C.c_void_p(done.cuda_event),
+                                         C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                         C.byref(mr))
+    assert rc == 0
+    done.synchronize()
+    torch.cuda.synchronize()
+    assert taken[0] > 0 and not blocks
+    assert np.array_equal(ids.numpy(), ri.cpu().numpy())
+    assert np.array_equal(f32_bits(d2.numpy()), f32_bits(rd.cpu().numpy()))
